@@ -1,0 +1,203 @@
+/*
+ * mkf_b200 -- C ABI of the B200 multi-key mult+relin library.
+ *
+ * This is the drop-in boundary for the reference's evaluator call
+ *     mkckks.Evaluator.MulRelinNew / Rescale, mkbfv.Evaluator.MulRelinNew,
+ *     and the MKF aggregate-fold CKKSCase/BFVCase.Run / paper MulRelinNew
+ * (ZhangChuanxin1/MKF, software/kklss/... and software/mkf/mkf_cpu/...).
+ * A Go host binds it through cgo; every argument is a
+ * plain pointer, size or scalar.  All entry points return an mkf_status;
+ * mkf_last_error() gives the message of the last failure on a context.
+ *
+ * Data layout (the reference's fixture order, software/mkf/mkf_cpu/
+ * fpga_fixture_test.go:3-5,45-69): little-endian uint64 words, component
+ * major, then limb (RNS modulus) major, then coefficient.  A switching key is
+ * [beta][2][nQ+nP][N] (Q limbs then P limbs), stored exactly as Lattigo
+ * stores rlwe.SwitchingKey: Montgomery form, NTT domain.
+ *
+ * Thread safety: a context may be used from several host threads when each
+ * thread uses its own stream; calls on one stream are ordered.
+ */
+#ifndef MKF_B200_H
+#define MKF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mkf_status {
+    MKF_OK = 0,
+    MKF_ERR_INVALID_ARG = 1,  /* bad handle, size, level or parameter */
+    MKF_ERR_CUDA = 2,         /* a CUDA call failed */
+    MKF_ERR_OOM = 3,          /* device memory exhausted */
+    MKF_ERR_UNSUPPORTED = 4,  /* parameter shape outside what is built */
+    MKF_ERR_MISSING_KEY = 5,  /* no key for a party of the operands */
+    MKF_ERR_LEVEL = 6,        /* level/scale precondition violated */
+    MKF_ERR_TIMEOUT = 7,      /* a bounded device or host wait expired */
+    MKF_ERR_BUSY = 8,         /* admission refused (server full) */
+    MKF_ERR_CANCELLED = 9     /* request cancelled before it ran */
+} mkf_status;
+
+enum { MKF_SCHEME_CKKS = 0, MKF_SCHEME_BFV = 1 };
+
+typedef struct mkf_ctx mkf_ctx;
+typedef struct mkf_key mkf_key;
+typedef struct mkf_ct mkf_ct;
+typedef struct mkf_mkf_keyset mkf_mkf_keyset;
+typedef struct mkf_kklss_keyset mkf_kklss_keyset;
+
+/* Parameters (replaces ckks.ParametersLiteral / bfv.ParametersLiteral /
+ * mkbfv.ParametersLiteral: software/mkf/mkf_cpu/params.go:15-101,
+ * software/kklss/mkbfv/params.go:116-185). */
+typedef struct mkf_params_desc {
+    int scheme;           /* MKF_SCHEME_CKKS or MKF_SCHEME_BFV */
+    int log_n;            /* ring degree N = 2^log_n */
+    const uint64_t *q;    /* Q chain, q[0] first */
+    int n_q;
+    const uint64_t *p;    /* special primes P */
+    int n_p;
+    const uint64_t *q_mul;/* BFV auxiliary chain QMul (len == n_q), or NULL */
+    int n_q_mul;
+    double scale;         /* CKKS default scale */
+    uint64_t t;           /* BFV plaintext modulus */
+    int device;           /* CUDA device ordinal */
+} mkf_params_desc;
+
+/* Creates a context (moduli, NTT and basis-extension tables in HBM).
+ * Replaces mkckks.NewParameters + NewEvaluator (software/kklss/mkckks/
+ * params.go:17, evaluator.go:24), mkbfv.NewParametersFromLiteral
+ * (mkbfv/params.go:140) and the MKF CKKSParameters/BFVParameters
+ * (mkf_cpu/params.go:102-143). */
+mkf_status mkf_ctx_create(const mkf_params_desc *desc, mkf_ctx **out);
+void mkf_ctx_destroy(mkf_ctx *ctx);
+/* Copies the last error message of ctx (NUL-terminated) into buf. */
+mkf_status mkf_last_error(const mkf_ctx *ctx, char *buf, size_t len);
+/* Beta (number of gadget digits) at `level` for gamma = 1 (Lattigo rlwe,
+ * MKF) or gamma = 2 (KKLSS), mkrlwe/params.go:63-71. */
+int mkf_ctx_beta(const mkf_ctx *ctx, int level, int gamma);
+/* Library version string. */
+const char *mkf_version(void);
+
+/* ------------------------------------------------------------------ */
+/* key material                                                        */
+/* ------------------------------------------------------------------ */
+enum {
+    /* rlwe.SwitchingKey [beta][2][nQ+nP][N] (MKF fold and relin keys,
+     * software/mkf/mkf_cpu/common.go:27-51) */
+    MKF_KEY_SWITCHING = 1,
+    /* mkrlwe.RelinearizationKey (b, d, v): [3][beta][nQ+nP][N]
+     * (software/kklss/mkrlwe/keys.go:131-136, keygen.go:137-187) */
+    MKF_KEY_KKLSS_RLK = 2,
+    /* mkbfv.RelinearizationKey, two (b, d, v) halves: [2][3][beta][nQ+nP][N]
+     * (software/kklss/mkbfv/keys.go:6-9) */
+    MKF_KEY_KKLSS_BFV_RLK = 3,
+    /* one gadget vector, e.g. the CRS u = CRS[-1]: [beta][nQ+nP][N]
+     * (software/kklss/mkrlwe/params.go:37-58) */
+    MKF_KEY_GADGET = 4
+};
+/* Words a key of `kind` occupies at full level. */
+size_t mkf_key_words(const mkf_ctx *ctx, int kind);
+/* Uploads key words from host memory into HBM. */
+mkf_status mkf_key_upload(mkf_ctx *ctx, int kind, const uint64_t *words, size_t n_words,
+                          mkf_key **out);
+void mkf_key_destroy(mkf_key *key);
+
+/* ------------------------------------------------------------------ */
+/* ciphertexts (HBM-resident)                                           */
+/* ------------------------------------------------------------------ */
+/* A ciphertext of n_comp polynomials at `level` (level+1 limbs each):
+ * component 0 is c0, component i >= 1 belongs to party ids[i-1]
+ * (mkrlwe.Ciphertext map ID->Poly, mkrlwe/elements.go:17-33; MKF
+ * multiCiphertext/outputCiphertext, mkf_cpu/common.go:10-25).  is_ntt
+ * records the domain as Lattigo's Poly.IsNTT does. */
+mkf_status mkf_ct_create(mkf_ctx *ctx, int n_comp, int level, int is_ntt, mkf_ct **out);
+void mkf_ct_destroy(mkf_ct *ct);
+mkf_status mkf_ct_set_parties(mkf_ct *ct, const int32_t *ids, int n);
+mkf_status mkf_ct_get_parties(const mkf_ct *ct, int32_t *ids, int cap, int *n);
+mkf_status mkf_ct_set_scale(mkf_ct *ct, double scale);
+double mkf_ct_scale(const mkf_ct *ct);
+int mkf_ct_level(const mkf_ct *ct);
+int mkf_ct_ncomp(const mkf_ct *ct);
+/* Host <-> HBM copies of all n_comp*(level+1)*N words.  stream may be NULL
+ * (context stream); the call returns after the copy completed. */
+mkf_status mkf_ct_upload(mkf_ct *ct, const uint64_t *host, size_t n_words, void *stream);
+mkf_status mkf_ct_download(const mkf_ct *ct, uint64_t *host, size_t n_words, void *stream);
+/* Asynchronous variants (host memory must be pinned and stay valid). */
+mkf_status mkf_ct_upload_async(mkf_ct *ct, const uint64_t *host, size_t n_words, void *stream);
+mkf_status mkf_ct_download_async(const mkf_ct *ct, uint64_t *host, size_t n_words, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* MKF aggregate-fold construction                                      */
+/* ------------------------------------------------------------------ */
+/* The online key bundle of one party subset: k fold keys s_i -> s_E and
+ * the relinearization key s_E^2 -> s_E (mkf_cpu/common.go:27-51). */
+mkf_status mkf_mkf_keyset_create(mkf_ctx *ctx, const mkf_key *const *fold, int k,
+                                 const mkf_key *relin, mkf_mkf_keyset **out);
+void mkf_mkf_keyset_destroy(mkf_mkf_keyset *ks);
+
+enum {
+    MKF_FLAG_RESCALE = 1,     /* CKKS: apply Rescale(params scale) after relin */
+    MKF_FLAG_MATERIALIZE = 2  /* write the (k+1)-component form: C0 + k x Gamma */
+};
+/* MKF mult+relin: fold both operands (k switches each), 2x2 Karatsuba
+ * tensor, one relinearization switch, optional rescale and
+ * materialization.  Replaces CKKSCase.Run (mkf_cpu/ckks.go:102-166),
+ * BFVCase.Run (mkf_cpu/bfv.go:212-252) and paperMKFCKKSEvaluator.MulRelinNew
+ * (mkf_cpu/true_mkf_ckks.go:253-304).  CKKS operands are in the NTT domain,
+ * BFV operands in the coefficient domain at full level.  `out` must have 2
+ * components (compact C0, Gamma) or k+1 with MKF_FLAG_MATERIALIZE, at the
+ * output level.  Asynchronous on `stream`. */
+mkf_status mkf_mkf_mulrelin(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
+                            const mkf_mkf_keyset *ks, int flags, mkf_ct *out, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* KKLSS per-party-key construction                                     */
+/* ------------------------------------------------------------------ */
+/* RelinearizationKeySet (mkrlwe/keys.go:151-156, 263-281) plus the CRS u. */
+mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out);
+mkf_status mkf_kklss_keyset_add(mkf_kklss_keyset *ks, int32_t party_id, const mkf_key *rlk);
+void mkf_kklss_keyset_destroy(mkf_kklss_keyset *ks);
+/* Output party list of a KKLSS product: op0's ids, then op1's ids not in
+ * op0 (the reference's IDSet union). */
+mkf_status mkf_kklss_union(const mkf_ct *op0, const mkf_ct *op1, int32_t *ids, int cap, int *n);
+/* KKLSS mult+relin (+ rescale for CKKS), coefficient-domain operands.
+ * Replaces mkckks.Evaluator.MulRelinNew (mkckks/evaluator.go:419-446,
+ * 561-586) and mkbfv.Evaluator.MulRelinNew (mkbfv/evaluator.go:85-152).
+ * `out` must have |union|+1 components at the output level; its party ids
+ * and scale are set.  Missing keys give MKF_ERR_MISSING_KEY. */
+mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
+                              const mkf_kklss_keyset *ks, mkf_ct *out, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* rescale and stage-level primitives                                   */
+/* ------------------------------------------------------------------ */
+/* Rescale by the last moduli while scale/q >= min_scale/2 (Lattigo
+ * ckks.Evaluator.Rescale; mkckks/evaluator.go:360-401).  Domain taken from
+ * the ciphertext's is_ntt.  out: same components, lower level. */
+mkf_status mkf_rescale(mkf_ctx *ctx, const mkf_ct *in, double min_scale, mkf_ct *out,
+                       void *stream);
+/* Host-buffer primitives (synchronous), for stage-level parity:
+ *   basis 0 = Q, 1 = P, 2 = QMul; limbs [first, first+n_limbs).           */
+mkf_status mkf_ntt_host(mkf_ctx *ctx, int basis, int first, int n_limbs, const uint64_t *in,
+                        uint64_t *out, int inverse);
+/* Gadget decomposition of a coefficient-domain Q polynomial at `level`
+ * (rlwe DecomposeNTT, gamma 1; mkrlwe Decompose, gamma 2).
+ * out: [beta][level+1+nP][N], NTT domain. */
+mkf_status mkf_decompose_host(mkf_ctx *ctx, int gamma, int level, const uint64_t *in,
+                              uint64_t *out);
+/* MKF switchOne (mkf_cpu/common.go:79-107). key: [beta][2][nQ+nP][N]. */
+mkf_status mkf_switch_one_host(mkf_ctx *ctx, int level, int in_ntt, const uint64_t *in,
+                               const uint64_t *key, int ntt_output, uint64_t *out0,
+                               uint64_t *out1);
+
+/* Number of this library's kernels launched on the calling thread since the
+ * last reset (instrumentation for the benchmark). */
+uint64_t mkf_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MKF_B200_H */

@@ -1,0 +1,134 @@
+"""ctypes binding of libmkf_b200.so (the C ABI in include/mkf_b200.h).
+
+The library is required: importing this module without the built extension
+raises, there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmkf_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mkf_b200.h")
+
+u64p = ctypes.POINTER(ctypes.c_uint64)
+i32p = ctypes.POINTER(ctypes.c_int32)
+vp = ctypes.c_void_p
+
+OK = 0
+STATUS = {
+    0: "MKF_OK", 1: "MKF_ERR_INVALID_ARG", 2: "MKF_ERR_CUDA", 3: "MKF_ERR_OOM",
+    4: "MKF_ERR_UNSUPPORTED", 5: "MKF_ERR_MISSING_KEY", 6: "MKF_ERR_LEVEL",
+    7: "MKF_ERR_TIMEOUT", 8: "MKF_ERR_BUSY", 9: "MKF_ERR_CANCELLED",
+}
+SCHEME = {"ckks": 0, "bfv": 1}
+KEY_SWITCHING, KEY_KKLSS_RLK, KEY_KKLSS_BFV_RLK, KEY_GADGET = 1, 2, 3, 4
+FLAG_RESCALE, FLAG_MATERIALIZE = 1, 2
+
+
+class MKFError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class MissingKeyError(MKFError):
+    pass
+
+
+class LevelError(MKFError):
+    pass
+
+
+class ParamsDesc(ctypes.Structure):
+    _fields_ = [
+        ("scheme", ctypes.c_int), ("log_n", ctypes.c_int),
+        ("q", u64p), ("n_q", ctypes.c_int),
+        ("p", u64p), ("n_p", ctypes.c_int),
+        ("q_mul", u64p), ("n_q_mul", ctypes.c_int),
+        ("scale", ctypes.c_double), ("t", ctypes.c_uint64), ("device", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def declared_symbols():
+    """Entry points declared in include/mkf_b200.h."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(mkf_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m mkf_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    i, d, sz = ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    sig = {
+        "mkf_version": (ctypes.c_char_p, []),
+        "mkf_launch_count": (ctypes.c_uint64, [i]),
+        "mkf_ctx_create": (i, [ctypes.POINTER(ParamsDesc), ctypes.POINTER(vp)]),
+        "mkf_ctx_destroy": (None, [vp]),
+        "mkf_last_error": (i, [vp, ctypes.c_char_p, sz]),
+        "mkf_ctx_beta": (i, [vp, i, i]),
+        "mkf_key_words": (sz, [vp, i]),
+        "mkf_key_upload": (i, [vp, i, u64p, sz, ctypes.POINTER(vp)]),
+        "mkf_key_destroy": (None, [vp]),
+        "mkf_ct_create": (i, [vp, i, i, i, ctypes.POINTER(vp)]),
+        "mkf_ct_destroy": (None, [vp]),
+        "mkf_ct_set_parties": (i, [vp, i32p, i]),
+        "mkf_ct_get_parties": (i, [vp, i32p, i, ctypes.POINTER(i)]),
+        "mkf_ct_set_scale": (i, [vp, d]),
+        "mkf_ct_scale": (d, [vp]),
+        "mkf_ct_level": (i, [vp]),
+        "mkf_ct_ncomp": (i, [vp]),
+        "mkf_ct_upload": (i, [vp, u64p, sz, vp]),
+        "mkf_ct_download": (i, [vp, u64p, sz, vp]),
+        "mkf_ct_upload_async": (i, [vp, u64p, sz, vp]),
+        "mkf_ct_download_async": (i, [vp, u64p, sz, vp]),
+        "mkf_mkf_keyset_create": (i, [vp, ctypes.POINTER(vp), i, vp, ctypes.POINTER(vp)]),
+        "mkf_mkf_keyset_destroy": (None, [vp]),
+        "mkf_mkf_mulrelin": (i, [vp, vp, vp, vp, i, vp, vp]),
+        "mkf_kklss_keyset_create": (i, [vp, vp, ctypes.POINTER(vp)]),
+        "mkf_kklss_keyset_add": (i, [vp, ctypes.c_int32, vp]),
+        "mkf_kklss_keyset_destroy": (None, [vp]),
+        "mkf_kklss_union": (i, [vp, vp, i32p, i, ctypes.POINTER(i)]),
+        "mkf_kklss_mulrelin": (i, [vp, vp, vp, vp, vp, vp]),
+        "mkf_rescale": (i, [vp, vp, d, vp, vp]),
+        "mkf_ntt_host": (i, [vp, i, i, i, u64p, u64p, i]),
+        "mkf_decompose_host": (i, [vp, i, i, u64p, u64p]),
+        "mkf_switch_one_host": (i, [vp, i, i, u64p, u64p, i, u64p, u64p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def ptr(a: np.ndarray):
+    if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous uint64 array")
+    return a.ctypes.data_as(u64p)
+
+
+def check(ctx_handle, status: int):
+    if status == OK:
+        return
+    buf = ctypes.create_string_buffer(512)
+    if ctx_handle:
+        lib().mkf_last_error(ctx_handle, buf, 512)
+    msg = buf.value.decode(errors="replace")
+    if status == 5:
+        raise MissingKeyError(status, msg)
+    if status == 6:
+        raise LevelError(status, msg)
+    raise MKFError(status, msg)

@@ -1,0 +1,605 @@
+// extern "C" entry points of libmkf_b200.so (declared in include/mkf_b200.h).
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mkf_b200.h"
+#include "eval.h"
+
+namespace mkf {
+std::atomic<uint64_t> g_launches{0};
+}
+
+using namespace mkf;
+
+struct mkf_ctx {
+    Context c;
+    cudaStream_t stream = nullptr;
+    std::mutex ws_mu;
+    std::map<cudaStream_t, std::unique_ptr<Workspace>> ws;
+    std::mutex err_mu;
+    std::string err;
+};
+
+struct mkf_key {
+    mkf_ctx *ctx = nullptr;
+    int kind = 0;
+    uint64_t *d = nullptr;
+    size_t words = 0;
+};
+
+struct mkf_ct {
+    mkf_ctx *ctx = nullptr;
+    int ncomp = 0, level = 0, is_ntt = 0;
+    double scale = 0;
+    std::vector<int32_t> ids;
+    uint64_t *d = nullptr;
+    size_t words() const { return (size_t)ncomp * (level + 1) * ctx->c.N; }
+    long long cs() const { return (long long)(level + 1) * ctx->c.N; }
+};
+
+struct mkf_mkf_keyset {
+    mkf_ctx *ctx = nullptr;
+    int k = 0;
+    std::vector<const uint64_t *> fold;
+    const uint64_t *relin = nullptr;
+};
+
+struct mkf_kklss_keyset {
+    mkf_ctx *ctx = nullptr;
+    const uint64_t *crs_u = nullptr;
+    std::map<int32_t, const mkf_key *> rlk;
+};
+
+namespace {
+
+mkf_status fail(mkf_ctx *ctx, mkf_status s, const std::string &msg) {
+    if (ctx) {
+        std::lock_guard<std::mutex> g(ctx->err_mu);
+        ctx->err = msg;
+    }
+    return s;
+}
+
+mkf_status cuda_check(mkf_ctx *ctx, const char *where) {
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return MKF_OK;
+    return fail(ctx, e == cudaErrorMemoryAllocation ? MKF_ERR_OOM : MKF_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+cudaStream_t pick(mkf_ctx *ctx, void *stream) {
+    return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+Workspace *workspace(mkf_ctx *ctx, cudaStream_t st) {
+    std::lock_guard<std::mutex> g(ctx->ws_mu);
+    auto &w = ctx->ws[st];
+    if (!w) {
+        w.reset(new Workspace());
+        w->device = ctx->c.device;
+    }
+    return w.get();
+}
+
+mkf_status status_of(const std::string &e) {
+    if (e.empty()) return MKF_OK;
+    if (e.find("level") != std::string::npos || e.find("rescale") != std::string::npos)
+        return MKF_ERR_LEVEL;
+    if (e.find("support") != std::string::npos || e.find("needs") != std::string::npos)
+        return MKF_ERR_UNSUPPORTED;
+    return MKF_ERR_INVALID_ARG;
+}
+
+// Sizes the scratch with a dry run, grows the stream's workspace, then runs.
+template <class F> mkf_status run(mkf_ctx *ctx, cudaStream_t st, F &&f) {
+    cudaSetDevice(ctx->c.device);
+    Workspace *w = workspace(ctx, st);
+    Arena dry;
+    dry.dry = true;
+    std::string e = f(dry);
+    if (!e.empty()) return fail(ctx, status_of(e), e);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    if (dry.peak > w->cap_words) {
+        if (cap != cudaStreamCaptureStatusNone)
+            return fail(ctx, MKF_ERR_INVALID_ARG,
+                        "workspace too small during stream capture; run the operation once first");
+        if (!w->reserve(dry.peak)) return fail(ctx, MKF_ERR_OOM, "workspace allocation failed");
+    }
+    Arena a = w->arena();
+    e = f(a);
+    if (!e.empty()) return fail(ctx, status_of(e), e);
+    return cuda_check(ctx, "kernel launch");
+}
+
+bool same_ids(const std::vector<int32_t> &a, const std::vector<int32_t> &b) { return a == b; }
+
+} // namespace
+
+extern "C" {
+
+const char *mkf_version(void) { return "mkf_b200 0.1 (sm_100a)"; }
+
+uint64_t mkf_launch_count(int reset) {
+    if (reset) return g_launches.exchange(0);
+    return g_launches.load();
+}
+
+mkf_status mkf_ctx_create(const mkf_params_desc *d, mkf_ctx **out) {
+    if (!d || !out) return MKF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!d->q || !d->p || d->n_q <= 0 || d->n_p <= 0) return MKF_ERR_INVALID_ARG;
+    if (d->scheme != MKF_SCHEME_CKKS && d->scheme != MKF_SCHEME_BFV) return MKF_ERR_INVALID_ARG;
+    if (d->scheme == MKF_SCHEME_BFV && (!d->q_mul || d->n_q_mul != d->n_q || d->t < 2))
+        return MKF_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MKF_ERR_CUDA;
+    if (d->device < 0 || d->device >= ndev) return MKF_ERR_INVALID_ARG;
+    mkf_ctx *ctx = new (std::nothrow) mkf_ctx();
+    if (!ctx) return MKF_ERR_OOM;
+    std::string e = ctx->c.init(d->scheme, d->log_n, d->q, d->n_q, d->p, d->n_p, d->q_mul,
+                                d->scheme == MKF_SCHEME_BFV ? d->n_q_mul : 0, d->scale, d->t,
+                                d->device);
+    if (!e.empty()) {
+        delete ctx;
+        return e.find("device") != std::string::npos ? MKF_ERR_CUDA : MKF_ERR_INVALID_ARG;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return MKF_ERR_CUDA;
+    }
+    *out = ctx;
+    return MKF_OK;
+}
+
+void mkf_ctx_destroy(mkf_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->c.device);
+    cudaDeviceSynchronize();
+    ctx->ws.clear();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+mkf_status mkf_last_error(const mkf_ctx *ctx, char *buf, size_t len) {
+    if (!ctx || !buf || !len) return MKF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(const_cast<mkf_ctx *>(ctx)->err_mu);
+    size_t n = std::min(len - 1, ctx->err.size());
+    std::memcpy(buf, ctx->err.data(), n);
+    buf[n] = 0;
+    return MKF_OK;
+}
+
+int mkf_ctx_beta(const mkf_ctx *ctx, int level, int gamma) {
+    if (!ctx || gamma < 1 || gamma > 2 || ctx->c.nP % gamma) return -1;
+    if (level < 0 || level >= ctx->c.nQ) return -1;
+    return ctx->c.beta_of(level, gamma);
+}
+
+size_t mkf_key_words(const mkf_ctx *ctx, int kind) {
+    if (!ctx) return 0;
+    const Context &c = ctx->c;
+    const size_t kq = (size_t)(c.nQ + c.nP) * c.N;
+    switch (kind) {
+    case MKF_KEY_SWITCHING: return (size_t)c.beta_of(c.nQ - 1, 1) * 2 * kq;
+    case MKF_KEY_KKLSS_RLK:
+        return c.nP % 2 ? 0 : (size_t)3 * c.beta_of(c.nQ - 1, 2) * kq;
+    case MKF_KEY_KKLSS_BFV_RLK:
+        return c.nP % 2 ? 0 : (size_t)6 * c.beta_of(c.nQ - 1, 2) * kq;
+    case MKF_KEY_GADGET: return c.nP % 2 ? 0 : (size_t)c.beta_of(c.nQ - 1, 2) * kq;
+    default: return 0;
+    }
+}
+
+mkf_status mkf_key_upload(mkf_ctx *ctx, int kind, const uint64_t *words, size_t n_words,
+                          mkf_key **out) {
+    if (!ctx || !words || !out) return MKF_ERR_INVALID_ARG;
+    *out = nullptr;
+    size_t need = mkf_key_words(ctx, kind);
+    if (!need) return fail(ctx, MKF_ERR_INVALID_ARG, "unknown key kind or shape");
+    if (n_words != need)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "key has " + std::to_string(n_words) + " words, expected " + std::to_string(need));
+    cudaSetDevice(ctx->c.device);
+    mkf_key *k = new (std::nothrow) mkf_key();
+    if (!k) return MKF_ERR_OOM;
+    k->ctx = ctx;
+    k->kind = kind;
+    k->words = need;
+    if (cudaMalloc(&k->d, need * 8) != cudaSuccess) {
+        delete k;
+        cudaGetLastError();
+        return fail(ctx, MKF_ERR_OOM, "key allocation failed");
+    }
+    if (cudaMemcpy(k->d, words, need * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(k->d);
+        delete k;
+        return fail(ctx, MKF_ERR_CUDA, "key upload failed");
+    }
+    *out = k;
+    return MKF_OK;
+}
+
+void mkf_key_destroy(mkf_key *key) {
+    if (!key) return;
+    cudaSetDevice(key->ctx->c.device);
+    cudaFree(key->d);
+    delete key;
+}
+
+mkf_status mkf_ct_create(mkf_ctx *ctx, int n_comp, int level, int is_ntt, mkf_ct **out) {
+    if (!ctx || !out) return MKF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (n_comp < 1 || n_comp > kMaxParties + 2 || level < 0 || level >= ctx->c.nQ)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "bad ciphertext shape");
+    cudaSetDevice(ctx->c.device);
+    mkf_ct *ct = new (std::nothrow) mkf_ct();
+    if (!ct) return MKF_ERR_OOM;
+    ct->ctx = ctx;
+    ct->ncomp = n_comp;
+    ct->level = level;
+    ct->is_ntt = is_ntt;
+    ct->scale = ctx->c.scale;
+    for (int i = 1; i < n_comp; ++i) ct->ids.push_back(i - 1);
+    if (cudaMalloc(&ct->d, ct->words() * 8) != cudaSuccess) {
+        delete ct;
+        cudaGetLastError();
+        return fail(ctx, MKF_ERR_OOM, "ciphertext allocation failed");
+    }
+    cudaMemsetAsync(ct->d, 0, ct->words() * 8, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    *out = ct;
+    return MKF_OK;
+}
+
+void mkf_ct_destroy(mkf_ct *ct) {
+    if (!ct) return;
+    cudaSetDevice(ct->ctx->c.device);
+    cudaFree(ct->d);
+    delete ct;
+}
+
+mkf_status mkf_ct_set_parties(mkf_ct *ct, const int32_t *ids, int n) {
+    if (!ct || (n && !ids) || n != ct->ncomp - 1) return MKF_ERR_INVALID_ARG;
+    std::vector<int32_t> v(ids, ids + n);
+    std::vector<int32_t> s = v;
+    std::sort(s.begin(), s.end());
+    if (std::adjacent_find(s.begin(), s.end()) != s.end())
+        return fail(ct->ctx, MKF_ERR_INVALID_ARG, "repeated party id");
+    ct->ids = v;
+    return MKF_OK;
+}
+
+mkf_status mkf_ct_get_parties(const mkf_ct *ct, int32_t *ids, int cap, int *n) {
+    if (!ct || !n) return MKF_ERR_INVALID_ARG;
+    *n = (int)ct->ids.size();
+    if (ids) std::copy_n(ct->ids.begin(), std::min(cap, *n), ids);
+    return MKF_OK;
+}
+
+mkf_status mkf_ct_set_scale(mkf_ct *ct, double scale) {
+    if (!ct) return MKF_ERR_INVALID_ARG;
+    ct->scale = scale;
+    return MKF_OK;
+}
+double mkf_ct_scale(const mkf_ct *ct) { return ct ? ct->scale : 0.0; }
+int mkf_ct_level(const mkf_ct *ct) { return ct ? ct->level : -1; }
+int mkf_ct_ncomp(const mkf_ct *ct) { return ct ? ct->ncomp : -1; }
+
+static mkf_status ct_copy(mkf_ct *ct, const uint64_t *host_in, uint64_t *host_out, size_t n_words,
+                          void *stream, bool sync) {
+    if (!ct || n_words != ct->words() || !(host_in || host_out)) return MKF_ERR_INVALID_ARG;
+    mkf_ctx *ctx = ct->ctx;
+    cudaSetDevice(ctx->c.device);
+    cudaStream_t st = pick(ctx, stream);
+    cudaError_t e = host_in ? cudaMemcpyAsync(ct->d, host_in, n_words * 8, cudaMemcpyHostToDevice, st)
+                            : cudaMemcpyAsync(host_out, ct->d, n_words * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && sync) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(ctx, MKF_ERR_CUDA, cudaGetErrorString(e));
+    return MKF_OK;
+}
+
+mkf_status mkf_ct_upload(mkf_ct *ct, const uint64_t *host, size_t n, void *stream) {
+    return ct_copy(ct, host, nullptr, n, stream, true);
+}
+mkf_status mkf_ct_download(const mkf_ct *ct, uint64_t *host, size_t n, void *stream) {
+    return ct_copy(const_cast<mkf_ct *>(ct), nullptr, host, n, stream, true);
+}
+mkf_status mkf_ct_upload_async(mkf_ct *ct, const uint64_t *host, size_t n, void *stream) {
+    return ct_copy(ct, host, nullptr, n, stream, false);
+}
+mkf_status mkf_ct_download_async(const mkf_ct *ct, uint64_t *host, size_t n, void *stream) {
+    return ct_copy(const_cast<mkf_ct *>(ct), nullptr, host, n, stream, false);
+}
+
+mkf_status mkf_mkf_keyset_create(mkf_ctx *ctx, const mkf_key *const *fold, int k,
+                                 const mkf_key *relin, mkf_mkf_keyset **out) {
+    if (!ctx || !out || !fold || !relin || k < 1 || k > kMaxParties) return MKF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (relin->kind != MKF_KEY_SWITCHING || relin->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "relinearization key must be a switching key");
+    mkf_mkf_keyset *ks = new (std::nothrow) mkf_mkf_keyset();
+    if (!ks) return MKF_ERR_OOM;
+    ks->ctx = ctx;
+    ks->k = k;
+    for (int i = 0; i < k; ++i) {
+        if (!fold[i] || fold[i]->kind != MKF_KEY_SWITCHING || fold[i]->ctx != ctx) {
+            delete ks;
+            return fail(ctx, MKF_ERR_MISSING_KEY, "fold key " + std::to_string(i) + " missing");
+        }
+        ks->fold.push_back(fold[i]->d);
+    }
+    ks->relin = relin->d;
+    *out = ks;
+    return MKF_OK;
+}
+
+void mkf_mkf_keyset_destroy(mkf_mkf_keyset *ks) { delete ks; }
+
+mkf_status mkf_mkf_mulrelin(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
+                            const mkf_mkf_keyset *ks, int flags, mkf_ct *out, void *stream) {
+    if (!ctx || !left || !right || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (ks->ctx != ctx || left->ctx != ctx || right->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const int k = ks->k;
+    if (left->ncomp != k + 1 || right->ncomp != k + 1)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
+    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
+    const int level = std::min(left->level, right->level);
+    int nb = 0;
+    double scale = left->scale * right->scale;
+    if (!bfv && (flags & MKF_FLAG_RESCALE)) {
+        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
+        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
+    }
+    const int lout = level - nb;
+    const int n_out = (flags & MKF_FLAG_MATERIALIZE) ? k + 1 : 2;
+    if (out->ncomp != n_out || out->level != lout)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(n_out) + " components at level " +
+                        std::to_string(lout));
+    if (!bfv && (!left->is_ntt || !right->is_ntt))
+        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF CKKS operands must be in the NTT domain");
+    if (bfv && (left->is_ntt || right->is_ntt))
+        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF BFV operands must be in the coefficient domain");
+    Operand L{left->d, left->cs(), left->ncomp, left->level};
+    Operand R{right->d, right->cs(), right->ncomp, right->level};
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) kp.p[i] = ks->fold[i];
+    cudaStream_t st = pick(ctx, stream);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return mkf_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, L, R, kp, ks->relin, nb,
+                            n_out, out->d, out->cs());
+    });
+    if (s == MKF_OK) {
+        out->scale = scale;
+        out->is_ntt = !bfv;
+        out->ids = left->ids;
+        if (n_out == 2) out->ids.resize(1);
+    }
+    return s;
+}
+
+mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out) {
+    if (!ctx || !crs_u || !out) return MKF_ERR_INVALID_ARG;
+    if (crs_u->kind != MKF_KEY_GADGET || crs_u->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "CRS u must be a gadget vector");
+    mkf_kklss_keyset *ks = new (std::nothrow) mkf_kklss_keyset();
+    if (!ks) return MKF_ERR_OOM;
+    ks->ctx = ctx;
+    ks->crs_u = crs_u->d;
+    *out = ks;
+    return MKF_OK;
+}
+
+mkf_status mkf_kklss_keyset_add(mkf_kklss_keyset *ks, int32_t party_id, const mkf_key *rlk) {
+    if (!ks || !rlk) return MKF_ERR_INVALID_ARG;
+    const int want = ks->ctx->c.scheme == MKF_SCHEME_BFV ? MKF_KEY_KKLSS_BFV_RLK : MKF_KEY_KKLSS_RLK;
+    if (rlk->kind != want || rlk->ctx != ks->ctx)
+        return fail(ks->ctx, MKF_ERR_INVALID_ARG, "relinearization key kind does not match the scheme");
+    ks->rlk[party_id] = rlk;
+    return MKF_OK;
+}
+
+void mkf_kklss_keyset_destroy(mkf_kklss_keyset *ks) { delete ks; }
+
+mkf_status mkf_kklss_union(const mkf_ct *op0, const mkf_ct *op1, int32_t *ids, int cap, int *n) {
+    if (!op0 || !op1 || !n) return MKF_ERR_INVALID_ARG;
+    std::vector<int32_t> u = op0->ids;
+    for (int32_t id : op1->ids)
+        if (std::find(u.begin(), u.end(), id) == u.end()) u.push_back(id);
+    *n = (int)u.size();
+    if (ids) std::copy_n(u.begin(), std::min(cap, *n), ids);
+    return MKF_OK;
+}
+
+mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
+                              const mkf_kklss_keyset *ks, mkf_ct *out, void *stream) {
+    if (!ctx || !op0 || !op1 || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (ks->ctx != ctx || op0->ctx != ctx || op1->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
+    if (op0->is_ntt || op1->is_ntt)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "KKLSS operands must be in the coefficient domain");
+    std::vector<int32_t> u = op0->ids;
+    for (int32_t id : op1->ids)
+        if (std::find(u.begin(), u.end(), id) == u.end()) u.push_back(id);
+    const int k = (int)u.size();
+    if (k < 1 || k > kMaxParties) return fail(ctx, MKF_ERR_INVALID_ARG, "party count out of range");
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) {
+        auto it = ks->rlk.find(u[i]);
+        if (it == ks->rlk.end())
+            return fail(ctx, MKF_ERR_MISSING_KEY,
+                        "there is no relinearization key with id " + std::to_string(u[i]));
+        kp.p[i] = it->second->d;
+    }
+    const int level = std::min(op0->level, op1->level);
+    int nb = 0;
+    double scale = op0->scale * op1->scale;
+    if (!bfv) {
+        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
+        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
+    }
+    const int lout = level - nb;
+    if (out->ncomp != k + 1 || out->level != lout)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(k + 1) + " components at level " +
+                        std::to_string(lout));
+    cudaStream_t st = pick(ctx, stream);
+    cudaSetDevice(ctx->c.device);
+    // align the operands to the union party list (absent components are zero)
+    std::vector<mkf_ct *> tmp;
+    auto align = [&](const mkf_ct *op, Operand &o) -> mkf_status {
+        if (op->ids == u) {
+            o = Operand{op->d, op->cs(), op->ncomp, op->level};
+            return MKF_OK;
+        }
+        mkf_ct *t = nullptr;
+        mkf_status s = mkf_ct_create(ctx, k + 1, level, 0, &t);
+        if (s != MKF_OK) return s;
+        tmp.push_back(t);
+        const long long w = (long long)(level + 1) * ctx->c.N;
+        cudaMemsetAsync(t->d, 0, t->words() * 8, st);
+        cudaMemcpy2DAsync(t->d, w * 8, op->d, op->cs() * 8, w * 8, 1, cudaMemcpyDeviceToDevice, st);
+        for (size_t i = 0; i < op->ids.size(); ++i) {
+            int pos = (int)(std::find(u.begin(), u.end(), op->ids[i]) - u.begin());
+            cudaMemcpyAsync(t->d + (long long)(pos + 1) * w, op->d + (long long)(i + 1) * op->cs(),
+                            w * 8, cudaMemcpyDeviceToDevice, st);
+        }
+        o = Operand{t->d, w, k + 1, level};
+        return MKF_OK;
+    };
+    Operand O0, O1;
+    mkf_status s = align(op0, O0);
+    if (s == MKF_OK) s = align(op1, O1);
+    if (s == MKF_OK) {
+        s = run(ctx, st, [&](Arena &a) {
+            return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, O0, O1, kp, ks->crs_u,
+                                  nb, out->d, out->cs());
+        });
+    }
+    if (!tmp.empty()) cudaStreamSynchronize(st);
+    for (mkf_ct *t : tmp) mkf_ct_destroy(t);
+    if (s == MKF_OK) {
+        out->ids = u;
+        out->scale = scale;
+        out->is_ntt = 0;
+    }
+    return s;
+}
+
+mkf_status mkf_rescale(mkf_ctx *ctx, const mkf_ct *in, double min_scale, mkf_ct *out,
+                       void *stream) {
+    if (!ctx || !in || !out) return MKF_ERR_INVALID_ARG;
+    if (min_scale <= 0) return fail(ctx, MKF_ERR_LEVEL, "cannot Rescale: minScale is 0");
+    if (in->scale == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot Rescale: ciphertext scale is 0");
+    if (in->level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot Rescale: input Ciphertext already at level 0");
+    double scale = in->scale;
+    int nb = rescale_count(ctx->c, in->level, min_scale, &scale);
+    if (out->ncomp != in->ncomp || out->level != in->level - nb)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(in->ncomp) + " components at level " +
+                        std::to_string(in->level - nb));
+    cudaStream_t st = pick(ctx, stream);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return rescale_polys(ctx->c, a, st, in->level, in->is_ntt, in->d, in->cs(), in->ncomp, nb,
+                             out->d, out->cs());
+    });
+    if (s == MKF_OK) {
+        out->scale = scale;
+        out->is_ntt = in->is_ntt;
+        out->ids = in->ids;
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer primitives
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    uint64_t *p = nullptr;
+    explicit DevBuf(size_t words) {
+        if (cudaMalloc(&p, std::max<size_t>(words, 1) * 8) != cudaSuccess) p = nullptr;
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+mkf_status mkf_ntt_host(mkf_ctx *ctx, int basis, int first, int n_limbs, const uint64_t *in,
+                        uint64_t *out, int inverse) {
+    if (!ctx || !in || !out || n_limbs <= 0 || first < 0) return MKF_ERR_INVALID_ARG;
+    const Context &c = ctx->c;
+    int nb = basis == 0 ? c.nQ : basis == 1 ? c.nP : basis == 2 ? c.nQM : 0;
+    int off = basis == 0 ? 0 : basis == 1 ? c.pidx(0) : c.qmidx(0);
+    if (first + n_limbs > nb) return fail(ctx, MKF_ERR_INVALID_ARG, "limb range out of basis");
+    cudaSetDevice(c.device);
+    size_t w = (size_t)n_limbs * c.N;
+    DevBuf b(w);
+    if (!b.p) return fail(ctx, MKF_ERR_OOM, "allocation failed");
+    cudaStream_t st = ctx->stream;
+    cudaMemcpyAsync(b.p, in, w * 8, cudaMemcpyHostToDevice, st);
+    LimbSet ls{b.p, (long long)w, n_limbs, n_limbs, off + first, 0};
+    if (inverse)
+        ntt_inverse(c, ls, 1, st);
+    else
+        ntt_forward(c, ls, 1, st);
+    cudaMemcpyAsync(out, b.p, w * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_check(ctx, "ntt");
+    return cuda_check(ctx, "ntt");
+}
+
+mkf_status mkf_decompose_host(mkf_ctx *ctx, int gamma, int level, const uint64_t *in,
+                              uint64_t *out) {
+    if (!ctx || !in || !out || gamma < 1 || gamma > 2) return MKF_ERR_INVALID_ARG;
+    const Context &c = ctx->c;
+    if (level < 0 || level >= c.nQ || c.nP % gamma)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "bad level or gamma");
+    cudaSetDevice(c.device);
+    const int beta = c.beta_of(level, gamma);
+    size_t win = (size_t)(level + 1) * c.N, wout = (size_t)beta * (level + 1 + c.nP) * c.N;
+    DevBuf bi(win), bo(wout);
+    if (!bi.p || !bo.p) return fail(ctx, MKF_ERR_OOM, "allocation failed");
+    cudaStream_t st = ctx->stream;
+    cudaMemcpyAsync(bi.p, in, win * 8, cudaMemcpyHostToDevice, st);
+    mkf_status s = run(ctx, st, [&](Arena &a) { return decompose_poly(c, a, st, gamma, level, bi.p, bo.p); });
+    if (s != MKF_OK) return s;
+    cudaMemcpyAsync(out, bo.p, wout * 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return cuda_check(ctx, "decompose");
+}
+
+mkf_status mkf_switch_one_host(mkf_ctx *ctx, int level, int in_ntt, const uint64_t *in,
+                               const uint64_t *key, int ntt_output, uint64_t *out0,
+                               uint64_t *out1) {
+    if (!ctx || !in || !key || !out0 || !out1) return MKF_ERR_INVALID_ARG;
+    const Context &c = ctx->c;
+    if (level < 0 || level >= c.nQ) return fail(ctx, MKF_ERR_INVALID_ARG, "bad level");
+    cudaSetDevice(c.device);
+    size_t w = (size_t)(level + 1) * c.N, wk = mkf_key_words(ctx, MKF_KEY_SWITCHING);
+    DevBuf bi(w), bk(wk), b0(w), b1(w);
+    if (!bi.p || !bk.p || !b0.p || !b1.p) return fail(ctx, MKF_ERR_OOM, "allocation failed");
+    cudaStream_t st = ctx->stream;
+    cudaMemcpyAsync(bi.p, in, w * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bk.p, key, wk * 8, cudaMemcpyHostToDevice, st);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return switch_one(c, a, st, level, in_ntt, bi.p, bk.p, ntt_output, b0.p, b1.p);
+    });
+    if (s != MKF_OK) return s;
+    cudaMemcpyAsync(out0, b0.p, w * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out1, b1.p, w * 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return cuda_check(ctx, "switch");
+}
+
+} // extern "C"

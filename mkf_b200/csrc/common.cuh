@@ -1,0 +1,115 @@
+// Shared device types and 64-bit modular arithmetic for the multi-key
+// mult+relin kernels (sm_100a, integer pipes only).
+//
+// Conventions follow the reference's arithmetic (Lattigo v2.3.0 as called
+// from software/kklss/mkrlwe and software/mkf/mkf_cpu): Montgomery
+// reduction MRed(x, y) = x*y*2^-64 mod q with qinv = q^-1 mod 2^64
+// (hardware/u55c/hls/kernels/par1_montgomery.hpp:5-26), and Shoup products
+// with precomputed w' = floor(w*2^64/q) (par1_mod_arith.hpp:98-118) for
+// twiddles.  Every stored polynomial is canonical ([0,q)) unless a kernel's
+// comment says otherwise.
+#pragma once
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mkf {
+
+// kernels launched by this library (reported by mkf_launch_count)
+extern std::atomic<uint64_t> g_launches;
+inline void note_launch(int n = 1) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+// One RNS modulus with the constants the kernels need.
+struct DevModulus {
+    uint64_t q;
+    uint64_t qinv;    // q^-1 mod 2^64 (Montgomery)
+    uint64_t mont1;   // 2^64 mod q     (MRed(x, mont1) = x mod q for any x)
+    uint64_t r2;      // 2^128 mod q    (MRed(x, r2) = MForm(x))
+    uint64_t ninv;    // N^-1 mod q
+    uint64_t ninv_sh; // Shoup companion of ninv
+    uint64_t last;    // psi^-1_rev[1] * N^-1 mod q (last inverse stage)
+    uint64_t last_sh;
+    double qd;        // (double)q, as the reference's float64 correction uses
+    uint64_t pad;
+};
+
+// A twiddle with its Shoup companion, loaded as one 16-byte word.
+struct Tw {
+    uint64_t w, ws;
+};
+
+// A set of limbs to transform/process: npolys polynomials, each with
+// `limbs` limbs of N words.  Limb l < nq uses modulus index q_first + l,
+// limb l >= nq uses p_first + (l - nq).
+struct LimbSet {
+    uint64_t *base;
+    long long poly_stride; // words between consecutive polynomials
+    int limbs;
+    int nq;
+    int q_first;
+    int p_first;
+    __host__ __device__ int mod_of(int l) const {
+        return l < nq ? q_first + l : p_first + (l - nq);
+    }
+};
+
+#define MKF_DEV __device__ __forceinline__
+
+MKF_DEV uint64_t mulhi64(uint64_t a, uint64_t b) { return __umul64hi(a, b); }
+
+// x*y*2^-64 mod q, canonical.
+MKF_DEV uint64_t mred(uint64_t x, uint64_t y, uint64_t q, uint64_t qinv) {
+    uint64_t lo = x * y, hi = __umul64hi(x, y);
+    uint64_t h = __umul64hi(lo * qinv, q);
+    uint64_t r = hi - h + q;
+    return r >= q ? r - q : r;
+}
+
+// Montgomery reduction of a 128-bit value (hi < q), canonical.
+MKF_DEV uint64_t mred128(uint64_t hi, uint64_t lo, uint64_t q, uint64_t qinv) {
+    uint64_t h = __umul64hi(lo * qinv, q);
+    uint64_t r = hi - h + q;
+    return r >= q ? r - q : r;
+}
+
+// x*w mod q in [0, 2q) for any 64-bit x (Shoup).
+MKF_DEV uint64_t shoup_lazy(uint64_t x, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t qh = __umul64hi(x, ws);
+    return x * w - qh * q;
+}
+MKF_DEV uint64_t shoup(uint64_t x, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t r = shoup_lazy(x, w, ws, q);
+    return r >= q ? r - q : r;
+}
+
+MKF_DEV uint64_t add_mod(uint64_t a, uint64_t b, uint64_t q) {
+    uint64_t s = a + b;
+    return s >= q ? s - q : s;
+}
+MKF_DEV uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t q) {
+    return a >= b ? a - b : a + q - b;
+}
+// [0,4q) -> [0,q)
+MKF_DEV uint64_t reduce4(uint64_t x, uint64_t q) {
+    uint64_t t2 = 2 * q;
+    x = x >= t2 ? x - t2 : x;
+    return x >= q ? x - q : x;
+}
+
+// 128-bit accumulator with the high word kept below q, so that a final
+// Montgomery reduction is canonical after any number of terms.
+struct Acc128 {
+    uint64_t lo, hi;
+    MKF_DEV void zero() { lo = 0; hi = 0; }
+    MKF_DEV void mac(uint64_t a, uint64_t b, uint64_t q) {
+        uint64_t pl = a * b, ph = __umul64hi(a, b);
+        uint64_t nl = lo + pl;
+        hi += ph + (nl < lo ? 1 : 0);
+        lo = nl;
+        hi = hi >= q ? hi - q : hi;
+    }
+};
+
+} // namespace mkf

@@ -1,0 +1,580 @@
+// Multi-key mult+relin algorithms (MKF aggregate fold and KKLSS per-party
+// keys, for CKKS and BFV) composed from the batched kernels.
+//
+// Every stage is launched once over all parties / digits / limbs of the
+// product (the reference loops over them one polynomial at a time), so each
+// launch carries enough independent work to fill the 148 SMs.
+#include "eval.h"
+
+#include <algorithm>
+
+namespace mkf {
+
+Workspace::~Workspace() {
+    if (buf) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaFree(buf);
+        cudaSetDevice(prev);
+    }
+}
+
+bool Workspace::reserve(size_t words) {
+    if (words <= cap_words) return true;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (buf) cudaFree(buf); // cudaFree waits for pending work on the device
+    buf = nullptr;
+    cap_words = 0;
+    size_t w = words + words / 8 + 1024;
+    bool ok = cudaMalloc(&buf, w * 8) == cudaSuccess;
+    if (ok)
+        cap_words = w;
+    else
+        buf = nullptr;
+    cudaSetDevice(prev);
+    return ok;
+}
+
+int rescale_count(const Context &c, int level, double min_scale, double *scale) {
+    int nb = 0;
+    while (level - nb >= 0 && *scale / (double)c.Q[level - nb] >= min_scale / 2) {
+        *scale /= (double)c.Q[level - nb];
+        ++nb;
+    }
+    return nb;
+}
+
+namespace {
+
+LimbSet lsq(uint64_t *p, long long stride, int L1, int q_first = 0) {
+    return LimbSet{p, stride, L1, L1, q_first, 0};
+}
+LimbSet lsqp(const Context &c, uint64_t *p, long long stride, int L1) {
+    return LimbSet{p, stride, L1 + c.nP, L1, 0, c.pidx(0)};
+}
+LimbSet lsp_of_qp(const Context &c, uint64_t *p, long long stride, int L1) {
+    return LimbSet{p + (long long)L1 * c.N, stride, c.nP, 0, 0, c.pidx(0)};
+}
+LimbSet lsr(const Context &c, uint64_t *p, long long stride) {
+    return LimbSet{p, stride, c.nQ + c.nQM, c.nQ, 0, c.qmidx(0)};
+}
+ModMap rmap(const Context &c) { return ModMap{c.nQ, 0, c.qmidx(0)}; }
+ModMap qmmap(const Context &c) { return ModMap{0, 0, c.qmidx(0)}; }
+
+void d2d2(uint64_t *dst, long long dst_stride, const uint64_t *src, long long src_stride,
+          long long words, int rows, cudaStream_t st) {
+    if (rows <= 0 || words <= 0) return;
+    cudaMemcpy2DAsync(dst, dst_stride * 8, src, src_stride * 8, words * 8, rows,
+                      cudaMemcpyDeviceToDevice, st);
+}
+
+// Prepares a ModDown of npolys QP accumulators (NTT domain, level L1):
+// tmp receives ModUp_{P->Q} of the P part, in the NTT domain when
+// ntt_output, else the whole accumulator is brought to the coefficient
+// domain first (software/kklss/mkrlwe/basis_extension.go:192-288).
+void moddown_prepare(const Context &c, cudaStream_t st, uint64_t *acc, long long acc_pstride,
+                     int npolys, int L1, int ntt_output, uint64_t *tmp) {
+    const long long poly = (long long)L1 * c.N;
+    if (ntt_output) {
+        ntt_inverse(c, lsp_of_qp(c, acc, acc_pstride, L1), npolys, st);
+    } else {
+        ntt_inverse(c, lsqp(c, acc, acc_pstride, L1), npolys, st);
+    }
+    launch_modup(c, c.p_to_q, acc + (long long)L1 * c.N, acc_pstride, tmp, poly, 0, L1, qmap(L1), 1,
+                 npolys, st);
+    if (ntt_output) ntt_forward(c, lsq(tmp, poly, L1), npolys, st);
+}
+
+CombineSpec pdown(const Context &c, const uint64_t *acc, long long acc_pstride, const uint64_t *tmp,
+                  long long tmp_pstride, uint64_t *out, long long out_pstride, int accumulate) {
+    CombineSpec s;
+    s.x = acc;
+    s.x_pstride = acc_pstride;
+    s.y = tmp;
+    s.y_pstride = tmp_pstride;
+    s.negc = c.d_neg_pinv_q;
+    s.out = out;
+    s.out_pstride = out_pstride;
+    s.accumulate = accumulate;
+    return s;
+}
+
+void fill_ones(uint8_t *p, int n, cudaStream_t st) { cudaMemsetAsync(p, 1, n, st); }
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// MKF
+// ---------------------------------------------------------------------------
+std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
+                         int level, const Operand &left, const Operand &right,
+                         const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,
+                         uint64_t *out, long long out_cs) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1, NQP = L1 + nP;
+    const bool bfv = scheme == kBFV;
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (level < 0 || level >= nQ) return "level out of range";
+    if (nP > 8) return "at most 8 special primes are supported";
+    if (bfv && (c.nQM != nQ || level != nQ - 1)) return "MKF BFV needs QMul and the full level";
+    if (!bfv && nb_rescale > level) return "cannot rescale below level 0";
+    if (left.ncomp < k + 1 || right.ncomp < k + 1) return "operand has fewer than k+1 components";
+    if (left.level < level || right.level < level) return "operand level below the product level";
+    if (n_out < 2) return "output needs at least two components";
+    const int beta = c.beta_of(level, 1);
+    const long long poly = (long long)L1 * N, qp = (long long)NQP * N;
+    const int nR = nQ + c.nQM;
+    const long long rp = (long long)nR * N;
+    const long long kk = k;
+
+    uint64_t *coeff = bfv ? nullptr : ar.take(2 * kk * poly);
+    uint64_t *dig = ar.take(2 * kk * beta * qp);
+    uint64_t *acc = ar.take(4 * kk * qp);
+    uint64_t *tmp = ar.take(4 * kk * poly);
+    uint64_t *F = ar.take(4 * poly);
+    uint64_t *mu = ar.take(3 * poly);
+    uint64_t *rcoef = bfv ? nullptr : ar.take(poly);
+    uint64_t *rdig = ar.take(beta * qp);
+    uint64_t *racc = ar.take(2 * qp);
+    uint64_t *rtmp = ar.take(2 * poly);
+    uint64_t *AB = bfv ? ar.take(4 * rp) : nullptr;
+    uint64_t *pq = bfv ? ar.take(2 * poly) : nullptr;
+    uint64_t *ym = bfv ? ar.take(2LL * c.nQM * N) : nullptr;
+    uint64_t *PR = bfv ? ar.take(3 * rp) : nullptr;
+    uint64_t *yq = bfv ? ar.take(3 * poly) : nullptr;
+    uint64_t *last = bfv ? nullptr : ar.take(2LL * N);
+    uint64_t *tr = bfv ? nullptr : ar.take(2 * poly);
+    if (ar.dry) return "";
+
+    // 1. gadget decomposition of every component of both operands
+    if (!bfv) {
+        d2d2(coeff, poly, left.data + left.cs, left.cs, poly, k, st);
+        d2d2(coeff + kk * poly, poly, right.data + right.cs, right.cs, poly, k, st);
+        ntt_inverse(c, lsq(coeff, poly, L1), 2 * k, st);
+        launch_decompose(c, coeff, poly, 0, level, 1, 0, beta, dig, qp, beta * qp, 2 * k, st);
+    } else {
+        launch_decompose(c, left.data + left.cs, left.cs, 0, level, 1, 0, beta, dig, qp, beta * qp,
+                         k, st);
+        launch_decompose(c, right.data + right.cs, right.cs, 0, level, 1, 0, beta,
+                         dig + kk * beta * qp, qp, beta * qp, k, st);
+    }
+    ntt_forward(c, lsqp(c, dig, qp, L1), 2 * k * beta, st);
+
+    // 2. fold key inner products: each key read once for both operands
+    IpArgs ip;
+    ip.A = dig;
+    ip.a_tstride = qp;
+    ip.a_gstride = beta * qp;
+    ip.a_istride = kk * beta * qp;
+    ip.use_bptr = 1;
+    for (int i = 0; i < k; ++i) ip.bptr[i] = fold.p[i];
+    ip.b_tstride = 2LL * (nQ + nP) * N;
+    ip.b_ostride = (long long)(nQ + nP) * N;
+    ip.b_qlimbs = nQ;
+    ip.out = acc;
+    ip.out_gstride = 4 * qp;
+    ip.out_istride = 2 * qp;
+    ip.out_ostride = qp;
+    ip.nterms = beta;
+    ip.nin = 2;
+    ip.nout = 2;
+    ip.groups = k;
+    ip.L1 = L1;
+    ip.nP = nP;
+    launch_ip(c, ip, st);
+
+    // 3. ModDown and fold: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1
+    moddown_prepare(c, st, acc, qp, 4 * k, L1, !bfv, tmp);
+    d2d2(F, 2 * poly, left.data, left.cs, poly, 1, st);
+    d2d2(F + 2 * poly, 2 * poly, right.data, right.cs, poly, 1, st);
+    cudaMemsetAsync(F + poly, 0, poly * 8, st);
+    cudaMemsetAsync(F + 3 * poly, 0, poly * 8, st);
+    {
+        CombineSpec s = pdown(c, acc, qp, tmp, poly, F, poly, 1);
+        s.x_tstride = 4 * qp;
+        s.y_tstride = 4 * poly;
+        s.terms = k;
+        launch_moddown_combine(c, s, L1, qmap(L1), 4, st);
+    }
+
+    uint64_t *mu0 = mu, *mu1 = mu + poly, *mu2 = mu + 2 * poly;
+    if (!bfv) {
+        // 4. Karatsuba tensor in the NTT domain
+        launch_karatsuba(c, F, F + poly, F + 2 * poly, F + 3 * poly, mu0, mu1, mu2, L1, qmap(L1), st);
+        // 5. relinearize mu2 with the aggregate key
+        d2d2(rcoef, poly, mu2, poly, poly, 1, st);
+        ntt_inverse(c, lsq(rcoef, poly, L1), 1, st);
+    } else {
+        // 4. BFV: lift the left fold into R, scale the right fold into R
+        uint64_t *A0 = AB, *B0 = AB + 2 * rp;
+        d2d2(A0, rp, F, poly, poly, 2, st);
+        launch_modup(c, c.q_to_qm, F, poly, A0 + poly, rp, 0, c.nQM, qmmap(c), 1, 2, st);
+        launch_mul_const(c, F + 2 * poly, poly, c.d_qm_mform_q, pq, poly, L1, qmap(L1), 2, st);
+        launch_modup(c, c.q_to_qm, pq, poly, ym, (long long)c.nQM * N, 0, c.nQM, qmmap(c), 1, 2, st);
+        {
+            CombineSpec s;
+            s.y = ym;
+            s.y_pstride = (long long)c.nQM * N;
+            s.negc = c.d_neg_qinv_qm;
+            s.out = B0 + poly;
+            s.out_pstride = rp;
+            launch_moddown_combine(c, s, c.nQM, qmmap(c), 2, st);
+        }
+        launch_modup(c, c.qm_to_q, B0 + poly, rp, B0, rp, 0, nQ, qmap(nQ), 1, 2, st);
+        ntt_forward(c, lsr(c, AB, rp), 4, st);
+        launch_karatsuba(c, AB, AB + rp, B0, B0 + rp, PR, PR + rp, PR + 2 * rp, nR, rmap(c), st);
+        // quantize: x t, INTT, ModDown QMul -> Q
+        launch_mul_const(c, PR, rp, c.d_t_mform_r, PR, rp, nR, rmap(c), 3, st);
+        ntt_inverse(c, lsr(c, PR, rp), 3, st);
+        launch_modup(c, c.qm_to_q, PR + poly, rp, yq, poly, 0, nQ, qmap(nQ), 1, 3, st);
+        {
+            CombineSpec s;
+            s.x = PR;
+            s.x_pstride = rp;
+            s.y = yq;
+            s.y_pstride = poly;
+            s.negc = c.d_neg_qminv_q;
+            s.out = mu;
+            s.out_pstride = poly;
+            launch_moddown_combine(c, s, nQ, qmap(nQ), 3, st);
+        }
+    }
+    // relinearization key switch of mu2 (coefficient domain input)
+    launch_decompose(c, bfv ? mu2 : rcoef, poly, 0, level, 1, 0, beta, rdig, qp, beta * qp, 1, st);
+    ntt_forward(c, lsqp(c, rdig, qp, L1), beta, st);
+    {
+        IpArgs r;
+        r.A = rdig;
+        r.a_tstride = qp;
+        r.B = relin;
+        r.b_tstride = 2LL * (nQ + nP) * N;
+        r.b_ostride = (long long)(nQ + nP) * N;
+        r.b_qlimbs = nQ;
+        r.out = racc;
+        r.out_ostride = qp;
+        r.nterms = beta;
+        r.nin = 1;
+        r.nout = 2;
+        r.groups = 1;
+        r.L1 = L1;
+        r.nP = nP;
+        launch_ip(c, r, st);
+    }
+    moddown_prepare(c, st, racc, qp, 2, L1, !bfv, rtmp);
+    launch_moddown_combine(c, pdown(c, racc, qp, rtmp, poly, mu, poly, 1), L1, qmap(L1), 2, st);
+
+    // 6. rescale (CKKS)
+    int lout = level;
+    for (int r = 0; r < nb_rescale; ++r) {
+        const int L = level - r;
+        d2d2(last, N, mu + (long long)L * N, poly, N, 2, st);
+        ntt_inverse(c, lsq(last, N, 1, L), 2, st);
+        launch_rescale_spread(c, last, N, L, tr, poly, 2, st);
+        ntt_forward(c, lsq(tr, poly, L), 2, st);
+        launch_rescale_combine(c, mu, poly, tr, poly, L, mu, poly, 2, st);
+        lout = L - 1;
+    }
+
+    // 7. output: C0, then Gamma (materialized n_out - 1 times)
+    const long long wout = (long long)(lout + 1) * N;
+    d2d2(out, out_cs, mu0, poly, wout, 1, st);
+    launch_replicate(mu1, out + out_cs, wout, n_out - 1, out_cs, st);
+    return "";
+}
+
+// ---------------------------------------------------------------------------
+// KKLSS
+// ---------------------------------------------------------------------------
+std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
+                           int level, const Operand &op0, const Operand &op1, const KeyPtrs &rlk,
+                           const uint64_t *crs_u, int nb_rescale, uint64_t *out, long long out_cs) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1, NQP = L1 + nP;
+    const bool bfv = scheme == kBFV;
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (nP % 2) return "KKLSS needs an even number of special primes";
+    if (nP / 2 > 8) return "at most 16 special primes are supported";
+    if (level < 0 || level >= nQ) return "level out of range";
+    if (bfv && (c.nQM != nQ || level != nQ - 1)) return "KKLSS BFV needs QMul and the full level";
+    if (bfv && nP != 2) return "KKLSS BFV supports two special primes (one-limb R digits)";
+    if (!bfv && nb_rescale > level) return "cannot rescale below level 0";
+    if (op0.ncomp < k + 1 || op1.ncomp < k + 1) return "operand has fewer than k+1 components";
+    if (op0.level < level || op1.level < level) return "operand level below the product level";
+    const int beta = c.beta_of(level, 2);
+    const int betaMax = c.beta_of(nQ - 1, 2);
+    const int nd = bfv ? 2 * beta : beta;
+    const long long poly = (long long)L1 * N, qp = (long long)NQP * N;
+    const long long kq = (long long)(nQ + nP) * N; // one full-level key polynomial
+    const long long vec = (long long)betaMax * kq;   // one gadget vector
+    const int nR = nQ + c.nQM;
+    const long long rp = (long long)nR * N;
+    const int K1 = k + 1;
+    const long long kk = k;
+    const long long tl = bfv ? rp : poly; // tensor operand stride
+
+    uint64_t *H0 = ar.take(2 * kk * nd * qp); // H0 then H1, adjacent
+    uint64_t *H1 = H0 + kk * nd * qp;
+    uint64_t *X = ar.take((long long)nd * qp);
+    uint64_t *Y = ar.take((long long)nd * qp);
+    uint64_t *T0 = ar.take(2 * K1 * tl); // T0 then T1, adjacent
+    uint64_t *T1 = T0 + K1 * tl;
+    uint64_t *CR = ar.take(K1 * tl);
+    uint64_t *CT = bfv ? ar.take(K1 * poly) : CR;
+    uint64_t *yq = bfv ? ar.take(K1 * poly) : nullptr;
+    uint64_t *E = ar.take(2 * kk * qp);
+    uint64_t *tmp = ar.take(2 * kk * poly);
+    uint64_t *Tq = ar.take(kk * poly);
+    uint64_t *G = ar.take(kk * beta * qp);
+    uint64_t *AR = bfv ? ar.take(K1 * rp) : nullptr;
+    uint64_t *BR = bfv ? ar.take(K1 * rp) : nullptr;
+    uint64_t *pq = bfv ? ar.take(K1 * poly) : nullptr;
+    uint64_t *ym = bfv ? ar.take(K1 * (long long)c.nQM * N) : nullptr;
+    uint64_t *trs = bfv ? nullptr : ar.take(K1 * poly);
+    uint8_t *ones = reinterpret_cast<uint8_t *>(ar.take(kMaxParties / 8 + 1));
+    if (ar.dry) return "";
+    fill_ones(ones, k, st);
+
+    // 1. operands in the decomposition ring, and their hoisted gadget digits
+    const uint64_t *d0, *d1;
+    long long d0s, d1s;
+    if (!bfv) {
+        d0 = op0.data + op0.cs;
+        d0s = op0.cs;
+        d1 = op1.data + op1.cs;
+        d1s = op1.cs;
+    } else {
+        // ModUpQtoR (mkbfv/basis_extension.go:50-66): Q copy + exact ModUp,
+        // keeping multSum's representatives (they are copied raw below)
+        d2d2(AR, rp, op0.data, op0.cs, poly, K1, st);
+        launch_modup(c, c.q_to_qm, op0.data, op0.cs, AR + poly, rp, 0, c.nQM, qmmap(c), 0, K1, st);
+        // conv.Rescale (mkbfv/basis_extension.go:88-104): floor(x QMul / Q) in R
+        launch_mul_const(c, op1.data, op1.cs, c.d_qm_mform_q, pq, poly, nQ, qmap(nQ), K1, st);
+        launch_modup(c, c.q_to_qm, pq, poly, ym, (long long)c.nQM * N, 0, c.nQM, qmmap(c), 1, K1, st);
+        {
+            CombineSpec s;
+            s.y = ym;
+            s.y_pstride = (long long)c.nQM * N;
+            s.negc = c.d_neg_qinv_qm;
+            s.out = BR + poly;
+            s.out_pstride = rp;
+            launch_moddown_combine(c, s, c.nQM, qmmap(c), K1, st);
+        }
+        launch_modup(c, c.qm_to_q, BR + poly, rp, BR, rp, 0, nQ, qmap(nQ), 0, K1, st);
+        d0 = AR + rp;
+        d0s = rp;
+        d1 = BR + rp;
+        d1s = rp;
+    }
+    launch_decompose(c, d0, d0s, bfv, level, 2, 0, nd, H0, qp, nd * qp, k, st);
+    launch_decompose(c, d1, d1s, bfv, level, 2, 0, nd, H1, qp, nd * qp, k, st);
+    ntt_forward(c, lsqp(c, H0, qp, L1), 2 * k * nd, st); // H0 and H1 are adjacent
+
+    // 2. x = MForm(sum_i d_i (.) g(op0_i)), y = MForm(sum_j b_j (.) g(op1_j))
+    //    (mkrlwe/keyswitch_hoisted.go:84-123; mkbfv/keyswitch_hoisted.go:100-148)
+    for (int half = 0; half < (bfv ? 2 : 1); ++half) {
+        for (int which = 0; which < 2; ++which) { // 0: x from d and op0; 1: y from b and op1
+            IpArgs ip;
+            ip.A = (which == 0 ? H0 : H1) + (long long)half * beta * qp;
+            ip.a_gstride = qp;
+            ip.a_tstride = (long long)nd * qp;
+            ip.use_bptr = 1;
+            ip.bptr_per_term = 1;
+            const long long off = (long long)(half * 3 + (which == 0 ? 1 : 0)) * vec;
+            for (int i = 0; i < k; ++i) ip.bptr[i] = rlk.p[i] + off;
+            ip.b_gstride = kq;
+            ip.b_qlimbs = nQ;
+            ip.out = (which == 0 ? X : Y) + (long long)half * beta * qp;
+            ip.out_gstride = qp;
+            ip.nterms = k;
+            ip.groups = beta;
+            ip.L1 = L1;
+            ip.nP = nP;
+            ip.mform_out = 1;
+            launch_ip(c, ip, st);
+        }
+    }
+
+    // 3. direct tensor terms (keyswitch_hoisted.go:126-153 / mkbfv 154-200)
+    if (!bfv) {
+        d2d2(T0, poly, op0.data, op0.cs, poly, K1, st);
+        d2d2(T1, poly, op1.data, op1.cs, poly, K1, st);
+        ntt_forward(c, lsq(T0, poly, L1), 2 * K1, st);
+        launch_kklss_tensor(c, T0, T1, CR, ones, ones, k, L1, qmap(L1), poly, st);
+        ntt_inverse(c, lsq(CR, poly, L1), K1, st);
+    } else {
+        d2d2(T0, rp, AR, rp, rp, K1, st);
+        d2d2(T1, rp, BR, rp, rp, K1, st);
+        ntt_forward(c, lsr(c, T0, rp), 2 * K1, st);
+        launch_kklss_tensor(c, T0, T1, CR, ones, ones, k, nR, rmap(c), rp, st);
+        launch_mul_const(c, CR, rp, c.d_t_mform_r, CR, rp, nR, rmap(c), K1, st);
+        ntt_inverse(c, lsr(c, CR, rp), K1, st);
+        launch_modup(c, c.qm_to_q, CR + poly, rp, yq, poly, 0, nQ, qmap(nQ), 1, K1, st);
+        CombineSpec s;
+        s.x = CR;
+        s.x_pstride = rp;
+        s.y = yq;
+        s.y_pstride = poly;
+        s.negc = c.d_neg_qminv_q;
+        s.out = CT;
+        s.out_pstride = poly;
+        launch_moddown_combine(c, s, nQ, qmap(nQ), K1, st);
+    }
+
+    // 4. ct_j += Ext(g(op1_j), x)
+    IpArgs ext;
+    ext.a_gstride = (long long)nd * qp;
+    ext.a_tstride = qp;
+    ext.b_tstride = qp;
+    ext.b_qlimbs = L1;
+    ext.out = E;
+    ext.out_gstride = qp;
+    ext.nterms = nd;
+    ext.groups = k;
+    ext.L1 = L1;
+    ext.nP = nP;
+    ext.A = H1;
+    ext.B = X;
+    launch_ip(c, ext, st);
+    moddown_prepare(c, st, E, qp, k, L1, 0, tmp);
+    launch_moddown_combine(c, pdown(c, E, qp, tmp, poly, CT + poly, poly, 1), L1, qmap(L1), k, st);
+
+    // 5. t_i = Ext(g(op0_i), y); ct_0 += Ext(g(t_i), v_i); ct_i += Ext(g(t_i), u)
+    ext.A = H0;
+    ext.B = Y;
+    launch_ip(c, ext, st);
+    moddown_prepare(c, st, E, qp, k, L1, 0, tmp);
+    launch_moddown_combine(c, pdown(c, E, qp, tmp, poly, Tq, poly, 0), L1, qmap(L1), k, st);
+    launch_decompose(c, Tq, poly, 0, level, 2, 0, beta, G, qp, beta * qp, k, st);
+    ntt_forward(c, lsqp(c, G, qp, L1), k * beta, st);
+    {
+        IpArgs v;
+        v.A = G;
+        v.a_gstride = beta * qp;
+        v.a_tstride = qp;
+        v.use_bptr = 1;
+        for (int i = 0; i < k; ++i) v.bptr[i] = rlk.p[i] + 2 * vec; // v of (the first half)
+        v.b_tstride = kq;
+        v.b_qlimbs = nQ;
+        v.out = E;
+        v.out_gstride = qp;
+        v.nterms = beta;
+        v.groups = k;
+        v.L1 = L1;
+        v.nP = nP;
+        launch_ip(c, v, st);
+        IpArgs u = v;
+        u.use_bptr = 0;
+        u.B = crs_u;
+        u.b_gstride = 0;
+        u.out = E + kk * qp;
+        launch_ip(c, u, st);
+    }
+    moddown_prepare(c, st, E, qp, 2 * k, L1, 0, tmp);
+    {
+        CombineSpec s = pdown(c, E, qp, tmp, poly, CT, poly, 1);
+        s.x_tstride = qp;
+        s.y_tstride = poly;
+        s.terms = k;
+        launch_moddown_combine(c, s, L1, qmap(L1), 1, st);
+    }
+    launch_moddown_combine(c, pdown(c, E + kk * qp, qp, tmp + kk * poly, poly, CT + poly, poly, 1),
+                           L1, qmap(L1), k, st);
+
+    // 6. rescale (CKKS, coefficient domain)
+    int lout = level;
+    for (int r = 0; r < nb_rescale; ++r) {
+        const int L = level - r;
+        launch_rescale_spread(c, CT + (long long)L * N, poly, L, trs, poly, K1, st);
+        launch_rescale_combine(c, CT, poly, trs, poly, L, CT, poly, K1, st);
+        lout = L - 1;
+    }
+    d2d2(out, out_cs, CT, poly, (long long)(lout + 1) * N, K1, st);
+    return "";
+}
+
+// ---------------------------------------------------------------------------
+// primitives
+// ---------------------------------------------------------------------------
+std::string switch_one(const Context &c, Arena &ar, cudaStream_t st, int level, int in_ntt,
+                       const uint64_t *in, const uint64_t *key, int ntt_output, uint64_t *out0,
+                       uint64_t *out1) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1, NQP = L1 + nP;
+    if (level < 0 || level >= nQ) return "level out of range";
+    if (nP > 8) return "at most 8 special primes are supported";
+    const int beta = c.beta_of(level, 1);
+    const long long poly = (long long)L1 * N, qp = (long long)NQP * N;
+    uint64_t *coeff = ar.take(poly);
+    uint64_t *dig = ar.take(beta * qp);
+    uint64_t *acc = ar.take(2 * qp);
+    uint64_t *tmp = ar.take(2 * poly);
+    if (ar.dry) return "";
+    d2d2(coeff, poly, in, poly, poly, 1, st);
+    if (in_ntt) ntt_inverse(c, lsq(coeff, poly, L1), 1, st);
+    launch_decompose(c, coeff, poly, 0, level, 1, 0, beta, dig, qp, beta * qp, 1, st);
+    ntt_forward(c, lsqp(c, dig, qp, L1), beta, st);
+    IpArgs r;
+    r.A = dig;
+    r.a_tstride = qp;
+    r.B = key;
+    r.b_tstride = 2LL * (nQ + nP) * N;
+    r.b_ostride = (long long)(nQ + nP) * N;
+    r.b_qlimbs = nQ;
+    r.out = acc;
+    r.out_ostride = qp;
+    r.nterms = beta;
+    r.nout = 2;
+    r.L1 = L1;
+    r.nP = nP;
+    launch_ip(c, r, st);
+    moddown_prepare(c, st, acc, qp, 2, L1, ntt_output, tmp);
+    launch_moddown_combine(c, pdown(c, acc, qp, tmp, poly, out0, poly, 0), L1, qmap(L1), 1, st);
+    launch_moddown_combine(c, pdown(c, acc + qp, qp, tmp + poly, poly, out1, poly, 0), L1, qmap(L1),
+                           1, st);
+    return "";
+}
+
+std::string rescale_polys(const Context &c, Arena &ar, cudaStream_t st, int level, int ntt,
+                          const uint64_t *in, long long in_cs, int npolys, int nb, uint64_t *out,
+                          long long out_cs) {
+    const int N = c.N, L1 = level + 1;
+    if (level < 0 || level >= c.nQ) return "level out of range";
+    if (nb < 0 || nb > level) return "cannot rescale below level 0";
+    const long long poly = (long long)L1 * N;
+    uint64_t *w = ar.take((long long)npolys * poly);
+    uint64_t *last = ar.take((long long)npolys * N);
+    uint64_t *t = ar.take((long long)npolys * poly);
+    if (ar.dry) return "";
+    d2d2(w, poly, in, in_cs, poly, npolys, st);
+    int lout = level;
+    for (int r = 0; r < nb; ++r) {
+        const int L = level - r;
+        if (ntt) {
+            d2d2(last, N, w + (long long)L * N, poly, N, npolys, st);
+            ntt_inverse(c, lsq(last, N, 1, L), npolys, st);
+            launch_rescale_spread(c, last, N, L, t, poly, npolys, st);
+            ntt_forward(c, lsq(t, poly, L), npolys, st);
+        } else {
+            launch_rescale_spread(c, w + (long long)L * N, poly, L, t, poly, npolys, st);
+        }
+        launch_rescale_combine(c, w, poly, t, poly, L, w, poly, npolys, st);
+        lout = L - 1;
+    }
+    d2d2(out, out_cs, w, poly, (long long)(lout + 1) * N, npolys, st);
+    return "";
+}
+
+std::string decompose_poly(const Context &c, Arena &ar, cudaStream_t st, int gamma, int level,
+                           const uint64_t *in_coeff, uint64_t *out) {
+    if (level < 0 || level >= c.nQ) return "level out of range";
+    if (c.nP % gamma) return "gamma must divide the number of special primes";
+    if (c.nP / gamma > 8) return "at most 8 limbs per digit are supported";
+    const int beta = c.beta_of(level, gamma);
+    const long long qp = (long long)(level + 1 + c.nP) * c.N;
+    if (ar.dry) return "";
+    launch_decompose(c, in_coeff, 0, 0, level, gamma, 0, beta, out, qp, beta * qp, 1, st);
+    ntt_forward(c, lsqp(c, out, qp, level + 1), beta, st);
+    return "";
+}
+
+} // namespace mkf

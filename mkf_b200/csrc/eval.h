@@ -1,0 +1,96 @@
+// Multi-key mult+relin algorithms on device-resident operands.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "ntt.h"
+
+namespace mkf {
+
+// Bump allocator over one device buffer.  In dry mode it only measures.
+struct Arena {
+    uint64_t *base = nullptr;
+    size_t cap = 0, used = 0, peak = 0;
+    bool dry = false;
+    uint64_t *take(size_t words) {
+        size_t w = (words + 31) & ~size_t(31); // 256-byte alignment
+        size_t off = used;
+        used += w;
+        if (used > peak) peak = used;
+        if (dry) return reinterpret_cast<uint64_t *>(uintptr_t(256) + off * 8);
+        return base + off;
+    }
+};
+
+// Per-stream scratch memory.
+struct Workspace {
+    int device = 0;
+    uint64_t *buf = nullptr;
+    size_t cap_words = 0;
+    ~Workspace();
+    // grows the buffer (never during stream capture); returns false on OOM
+    bool reserve(size_t words);
+    Arena arena() const {
+        Arena a;
+        a.base = buf;
+        a.cap = cap_words;
+        return a;
+    }
+};
+
+// ncomp polynomials of level+1 limbs; component c at data + c*cs
+struct Operand {
+    const uint64_t *data = nullptr;
+    long long cs = 0;
+    int ncomp = 0;
+    int level = 0;
+};
+
+struct KeyPtrs {
+    int k = 0;
+    const uint64_t *p[kMaxParties] = {};
+};
+
+enum : int { kCKKS = 0, kBFV = 1 };
+
+// All functions return "" on success or an error message.  With ar.dry they
+// only size the scratch they need.
+
+// MKF aggregate-fold mult+relin (software/mkf/mkf_cpu/ckks.go:102-166 and
+// bfv.go:212-252).  left/right: C0 + k components at `level` (CKKS: NTT
+// domain; BFV: coefficient domain, full level).  fold: per-party switching
+// keys s_i -> s_E ([betaMax][2][nQ+nP][N], MForm/NTT), relin: s_E^2 -> s_E.
+// Output: n_out components (C0, Gamma, then Gamma repeated to fill the
+// paper's (k+1)-component interface when n_out > 2) at level - nb_rescale.
+std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
+                         int level, const Operand &left, const Operand &right,
+                         const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,
+                         uint64_t *out, long long out_cs);
+
+// KKLSS mult+relin with per-party (b, d, v) keys (software/kklss/mkckks/
+// evaluator.go:419-446,561-586; software/kklss/mkbfv/evaluator.go:85-152).
+// op0/op1: component 0 then one component per party of the union party set
+// (absent components are zero), coefficient domain.  rlk.p[i]: CKKS
+// [3][betaMax][nQ+nP][N], BFV [2][3][betaMax][nQ+nP][N]; crs_u:
+// [betaMax][nQ+nP][N].  Output k+1 components at level - nb_rescale (CKKS).
+std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
+                           int level, const Operand &op0, const Operand &op1, const KeyPtrs &rlk,
+                           const uint64_t *crs_u, int nb_rescale, uint64_t *out, long long out_cs);
+
+// Stand-alone primitives (used by the C ABI and the stage-level tests).
+std::string switch_one(const Context &c, Arena &ar, cudaStream_t st, int level, int in_ntt,
+                       const uint64_t *in, const uint64_t *key, int ntt_output, uint64_t *out0,
+                       uint64_t *out1);
+std::string rescale_polys(const Context &c, Arena &ar, cudaStream_t st, int level, int ntt,
+                          const uint64_t *in, long long in_cs, int npolys, int nb, uint64_t *out,
+                          long long out_cs);
+std::string decompose_poly(const Context &c, Arena &ar, cudaStream_t st, int gamma, int level,
+                           const uint64_t *in_coeff, uint64_t *out);
+
+// Number of rescales Lattigo's Rescale loop performs (mkckks/evaluator.go:
+// 381-387): divide while scale / q_level >= min_scale / 2.
+int rescale_count(const Context &c, int level, double min_scale, double *scale);
+
+} // namespace mkf

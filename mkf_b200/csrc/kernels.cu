@@ -1,0 +1,455 @@
+// Element-wise and basis-extension kernels of the mult+relin path: gadget
+// decomposition (ModUp with the reference's float64 correction), key-switch
+// inner products, ModDown, tensor products and rescale.  All are streaming
+// kernels: one thread per coefficient, coalesced 8-byte accesses along the
+// coefficient axis, limbs / digits / polynomials on the other grid axes.
+#include "kernels.h"
+
+#include <algorithm>
+
+namespace mkf {
+
+constexpr int kBlock = 256;
+
+static inline dim3 grid_for(int N, int y = 1, int z = 1) {
+    return dim3((N + kBlock - 1) / kBlock, y, z);
+}
+
+// ----------------------------------------------------------------------------
+// exact basis extension pieces (software/kklss/mkrlwe/basis_extension.go)
+// ----------------------------------------------------------------------------
+
+// reconstructRNS (basis_extension.go:537-579): y_i = MRed(x_i, inv_i) and the
+// correction v = floor(sum_i y_i / q_i) in IEEE double, in the reference's
+// order, with explicit round-to-nearest intrinsics so that nothing is
+// reassociated or contracted.
+template <int MAXNS>
+MKF_DEV uint64_t reconstruct(const uint64_t *x, const ModUpTab &tab, const DevModulus *mods,
+                             uint64_t *y) {
+    double vi = 0.0;
+#pragma unroll
+    for (int i = 0; i < MAXNS; ++i) {
+        if (i < tab.ns) {
+            const DevModulus &m = mods[tab.src_mod[i]];
+            y[i] = mred(x[i], tab.inv[i], m.q, m.qinv);
+            vi = __dadd_rn(vi, __ddiv_rn(__ull2double_rn(y[i]), m.qd));
+        }
+    }
+    return __double2ull_rz(vi);
+}
+
+// multSum (basis_extension.go:581-646): sum y_i * qmod_i on 128 bits, lazy
+// Montgomery reduction, plus v*(-Q mod p).  Returns the exact representative
+// the reference produces.
+template <int MAXNS>
+MKF_DEV uint64_t multsum(const uint64_t *y, const ModUpTab &tab, int row, uint64_t v,
+                         const DevModulus &pm) {
+    const uint64_t *qm = tab.qmod + (size_t)row * tab.ns;
+    uint64_t lo = 0, hi = 0;
+#pragma unroll
+    for (int i = 0; i < MAXNS; ++i) {
+        if (i < tab.ns) {
+            const uint64_t b = qm[i];
+            const uint64_t pl = y[i] * b, ph = __umul64hi(y[i], b);
+            const uint64_t nl = lo + pl;
+            hi += ph + (nl < lo ? 1 : 0);
+            lo = nl;
+        }
+    }
+    const uint64_t h = __umul64hi(lo * pm.qinv, pm.q);
+    return hi - h + pm.q + tab.vq[(size_t)row * (tab.ns + 1) + v];
+}
+
+MKF_DEV uint64_t canon(uint64_t x, uint64_t q) {
+    while (x >= q) x -= q;
+    return x;
+}
+
+// ----------------------------------------------------------------------------
+// gadget decomposition
+// ----------------------------------------------------------------------------
+struct DecompArgs {
+    const uint64_t *in;
+    long long in_pstride;
+    uint64_t *out;
+    long long out_dstride, out_pstride;
+    const ModUpTab *tabs; // [digit][alpha+1]
+    const DevModulus *mods;
+    int level, alpha, digit0, nQ, nP, N, pmod0;
+};
+
+__global__ void __launch_bounds__(kBlock) decompose_kernel(DecompArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= a.N) return;
+    const int d = a.digit0 + blockIdx.y;
+    const uint64_t *in = a.in + (long long)blockIdx.z * a.in_pstride;
+    uint64_t *dst = a.out + (long long)blockIdx.z * a.out_pstride + (long long)blockIdx.y * a.out_dstride;
+    const int start = d * a.alpha;
+    int dl;
+    if (a.level > a.alpha * (d + 1) - 1)
+        dl = a.alpha - 2;
+    else
+        dl = (a.level % a.alpha) - 1;
+    const int ns = dl + 2;
+    const int L1 = a.level + 1;
+    if (ns == 1) {
+        // the single source limb is copied raw into every Q and P limb
+        const uint64_t v = in[(long long)start * a.N + x];
+        for (int j = 0; j < L1; ++j) {
+            const DevModulus &m = a.mods[j];
+            dst[(long long)j * a.N + x] = mred(v, m.mont1, m.q, m.qinv);
+        }
+        for (int j = 0; j < a.nP; ++j) {
+            const DevModulus &m = a.mods[a.pmod0 + j];
+            dst[(long long)(L1 + j) * a.N + x] = mred(v, m.mont1, m.q, m.qinv);
+        }
+        return;
+    }
+    const ModUpTab tab = a.tabs[d * (a.alpha + 1) + ns];
+    uint64_t xs[8], y[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < ns) xs[i] = in[(long long)(start + i) * a.N + x];
+    const uint64_t v = reconstruct<8>(xs, tab, a.mods, y);
+    for (int j = 0; j < L1; ++j) {
+        const DevModulus &m = a.mods[j];
+        uint64_t r;
+        if (j >= start && j < start + ns)
+            r = canon(xs[j - start], m.q);
+        else
+            r = canon(multsum<8>(y, tab, j, v, m), m.q);
+        dst[(long long)j * a.N + x] = r;
+    }
+    for (int j = 0; j < a.nP; ++j) {
+        const DevModulus &m = a.mods[a.pmod0 + j];
+        dst[(long long)(L1 + j) * a.N + x] = canon(multsum<8>(y, tab, a.nQ + j, v, m), m.q);
+    }
+}
+
+void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
+                      int level, int gamma, int digit0, int ndigits, uint64_t *out,
+                      long long out_dstride, long long out_pstride, int npolys, cudaStream_t st) {
+    if (ndigits <= 0 || npolys <= 0) return;
+    DecompArgs a;
+    a.in = in;
+    a.in_pstride = in_pstride;
+    a.out = out;
+    a.out_dstride = out_dstride;
+    a.out_pstride = out_pstride;
+    a.tabs = ring_r ? nullptr : c.d_decomp[gamma - 1];
+    a.mods = c.d_mods;
+    a.level = level;
+    a.alpha = c.alpha_of(gamma);
+    a.digit0 = digit0;
+    a.nQ = c.nQ;
+    a.nP = c.nP;
+    a.N = c.N;
+    a.pmod0 = c.pidx(0);
+    note_launch();
+    decompose_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(a);
+}
+
+// ----------------------------------------------------------------------------
+// inner products
+// ----------------------------------------------------------------------------
+template <int NIN, int NOUT>
+__global__ void __launch_bounds__(kBlock) ip_kernel(IpArgs a, const DevModulus *mods, int N,
+                                                     int pmod0) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int l = blockIdx.y, g = blockIdx.z;
+    const bool isq = l < a.L1;
+    const DevModulus m = mods[isq ? l : pmod0 + (l - a.L1)];
+    const long long aoff = (long long)g * a.a_gstride + (long long)l * N + x;
+    const long long blimb = (long long)(isq ? l : a.b_qlimbs + (l - a.L1)) * N + x;
+    // B addressing: default B + g*b_gstride + t*b_tstride; per-group pointers
+    // bptr[g] + t*b_tstride; per-term pointers bptr[t] + g*b_gstride
+    const long long boff = (a.use_bptr && !a.bptr_per_term ? 0 : (long long)g * a.b_gstride) + blimb;
+    const uint64_t *Bg = a.use_bptr && !a.bptr_per_term ? a.bptr[g] : a.B;
+    Acc128 acc[NIN][NOUT];
+#pragma unroll
+    for (int i = 0; i < NIN; ++i)
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) acc[i][o].zero();
+    for (int t = 0; t < a.nterms; ++t) {
+        uint64_t bv[NOUT];
+        const uint64_t *bp = (a.bptr_per_term ? a.bptr[t] : Bg) + boff +
+                             (a.bptr_per_term ? 0 : (long long)t * a.b_tstride);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) bv[o] = bp[(long long)o * a.b_ostride];
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) {
+            const uint64_t av = a.A[aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride];
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av, bv[o], m.q);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NIN; ++i)
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) {
+            uint64_t r = mred128(acc[i][o].hi, acc[i][o].lo, m.q, m.qinv);
+            if (a.mform_out) r = mred(r, m.r2, m.q, m.qinv);
+            uint64_t *op = a.out + (long long)g * a.out_gstride + (long long)i * a.out_istride +
+                           (long long)o * a.out_ostride + (long long)l * N + x;
+            if (a.accumulate) r = add_mod(*op, r, m.q);
+            *op = r;
+        }
+}
+
+void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
+    if (a.groups <= 0 || a.nterms < 0) return;
+    dim3 grid = grid_for(c.N, a.L1 + a.nP, a.groups);
+    const int pm = c.pidx(0);
+    note_launch();
+    if (a.nin == 1 && a.nout == 1)
+        ip_kernel<1, 1><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 1 && a.nout == 2)
+        ip_kernel<1, 2><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 2 && a.nout == 2)
+        ip_kernel<2, 2><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 2 && a.nout == 1)
+        ip_kernel<2, 1><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+}
+
+// ----------------------------------------------------------------------------
+// generic exact ModUp
+// ----------------------------------------------------------------------------
+struct ModUpArgs {
+    ModUpTab tab;
+    const uint64_t *src;
+    long long src_pstride;
+    uint64_t *out;
+    long long out_pstride;
+    const DevModulus *mods;
+    ModMap tgt;
+    int row0, nt, N, canonical;
+};
+
+template <int MAXNS>
+__global__ void __launch_bounds__(kBlock) modup_kernel(ModUpArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= a.N) return;
+    const uint64_t *src = a.src + (long long)blockIdx.y * a.src_pstride;
+    uint64_t *out = a.out + (long long)blockIdx.y * a.out_pstride;
+    uint64_t xs[MAXNS], y[MAXNS];
+#pragma unroll
+    for (int i = 0; i < MAXNS; ++i)
+        if (i < a.tab.ns) xs[i] = src[(long long)i * a.N + x];
+    const uint64_t v = reconstruct<MAXNS>(xs, a.tab, a.mods, y);
+    for (int j = 0; j < a.nt; ++j) {
+        const DevModulus &m = a.mods[a.tgt(j)];
+        uint64_t r = multsum<MAXNS>(y, a.tab, a.row0 + j, v, m);
+        if (a.canonical) r = canon(r, m.q);
+        out[(long long)j * a.N + x] = r;
+    }
+}
+
+void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, long long src_pstride,
+                  uint64_t *out, long long out_pstride, int row0, int nt, ModMap tgt, int canonical,
+                  int npolys, cudaStream_t st) {
+    if (npolys <= 0) return;
+    ModUpArgs a{tab, src, src_pstride, out, out_pstride, c.d_mods, tgt, row0, nt, c.N, canonical};
+    dim3 grid = grid_for(c.N, npolys);
+    note_launch();
+    if (tab.ns <= 4)
+        modup_kernel<4><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 8)
+        modup_kernel<8><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 16)
+        modup_kernel<16><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 32)
+        modup_kernel<32><<<grid, kBlock, 0, st>>>(a);
+    else
+        modup_kernel<64><<<grid, kBlock, 0, st>>>(a);
+}
+
+// ----------------------------------------------------------------------------
+// ModDown combine
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) moddown_combine_kernel(CombineSpec a, ModMap mm,
+                                                                  const DevModulus *mods, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y, p = blockIdx.z;
+    const DevModulus m = mods[mm(l)];
+    const uint64_t c = a.negc[l];
+    const long long o = (long long)l * N + i;
+    const long long xo = (long long)p * a.x_pstride + o, yo = (long long)p * a.y_pstride + o;
+    uint64_t r = 0;
+    for (int t = 0; t < a.terms; ++t) {
+        const uint64_t xv = a.x ? a.x[xo + (long long)t * a.x_tstride] : 0;
+        const uint64_t yv = a.y[yo + (long long)t * a.y_tstride];
+        r = add_mod(r, mred(yv + 2 * m.q - xv, c, m.q, m.qinv), m.q);
+    }
+    uint64_t *op = a.out + (long long)p * a.out_pstride + o;
+    if (a.accumulate) r = add_mod(*op, r, m.q);
+    *op = r;
+}
+
+void launch_moddown_combine(const Context &c, const CombineSpec &s, int nl, ModMap mm, int npolys,
+                            cudaStream_t st) {
+    if (npolys <= 0 || nl <= 0) return;
+    note_launch();
+    moddown_combine_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(s, mm, c.d_mods, c.N);
+}
+
+// ----------------------------------------------------------------------------
+// tensor products and element-wise helpers
+// ----------------------------------------------------------------------------
+MKF_DEV uint64_t mulmod_dev(uint64_t a, uint64_t b, const DevModulus &m) {
+    return mred(mred(a, m.r2, m.q, m.qinv), b, m.q, m.qinv);
+}
+
+__global__ void karatsuba_kernel(const uint64_t *a0, const uint64_t *a1, const uint64_t *b0,
+                                 const uint64_t *b1, uint64_t *mu0, uint64_t *mu1, uint64_t *mu2,
+                                 const DevModulus *mods, ModMap mm, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y;
+    const DevModulus m = mods[mm(l)];
+    const long long o = (long long)l * N + i;
+    const uint64_t x0 = a0[o], x1 = a1[o], y0 = b0[o], y1 = b1[o];
+    const uint64_t p0 = mulmod_dev(x0, y0, m);
+    const uint64_t p2 = mulmod_dev(x1, y1, m);
+    const uint64_t p1 = mulmod_dev(add_mod(x0, x1, m.q), add_mod(y0, y1, m.q), m);
+    mu0[o] = p0;
+    mu2[o] = p2;
+    mu1[o] = sub_mod(sub_mod(p1, p0, m.q), p2, m.q);
+}
+
+void launch_karatsuba(const Context &c, const uint64_t *a0, const uint64_t *a1, const uint64_t *b0,
+                      const uint64_t *b1, uint64_t *mu0, uint64_t *mu1, uint64_t *mu2, int nl,
+                      ModMap mm, cudaStream_t st) {
+    note_launch();
+    karatsuba_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(a0, a1, b0, b1, mu0, mu1, mu2, c.d_mods,
+                                                            mm, c.N);
+}
+
+__global__ void kklss_tensor_kernel(const uint64_t *a, const uint64_t *b, uint64_t *out,
+                                    const unsigned char *has0, const unsigned char *has1,
+                                    const DevModulus *mods, ModMap mm, int N, long long cs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y, j = blockIdx.z; // component j in [0, k]
+    const DevModulus m = mods[mm(l)];
+    const long long o = (long long)l * N + i;
+    const uint64_t a0 = a[o], b0 = b[o];
+    uint64_t r;
+    if (j == 0) {
+        r = mulmod_dev(a0, b0, m);
+    } else {
+        r = 0;
+        if (has0[j - 1]) r = mulmod_dev(b0, a[(long long)j * cs + o], m);
+        if (has1[j - 1]) r = add_mod(r, mulmod_dev(a0, b[(long long)j * cs + o], m), m.q);
+    }
+    out[(long long)j * cs + o] = r;
+}
+
+void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                         const unsigned char *d_has0, const unsigned char *d_has1, int k, int nl,
+                         ModMap mm, long long comp_stride, cudaStream_t st) {
+    note_launch();
+    kklss_tensor_kernel<<<grid_for(c.N, nl, k + 1), kBlock, 0, st>>>(a, b, out, d_has0, d_has1,
+                                                                      c.d_mods, mm, c.N,
+                                                                      comp_stride);
+}
+
+__global__ void mul_const_kernel(const uint64_t *x, long long xps, const uint64_t *cst,
+                                 uint64_t *out, long long ops, const DevModulus *mods, ModMap mm,
+                                 int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y, p = blockIdx.z;
+    const DevModulus m = mods[mm(l)];
+    const long long o = (long long)l * N + i;
+    out[(long long)p * ops + o] = mred(x[(long long)p * xps + o], cst[l], m.q, m.qinv);
+}
+
+void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
+                      const uint64_t *mform_const, uint64_t *out, long long out_pstride, int nl,
+                      ModMap mm, int npolys, cudaStream_t st) {
+    note_launch();
+    mul_const_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(x, x_pstride, mform_const, out,
+                                                                   out_pstride, c.d_mods, mm, c.N);
+}
+
+__global__ void add_kernel(uint64_t *acc, const uint64_t *x, const DevModulus *mods, ModMap mm,
+                           int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y;
+    const uint64_t q = mods[mm(l)].q;
+    const long long o = (long long)l * N + i;
+    acc[o] = add_mod(acc[o], x[o], q);
+}
+
+void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModMap mm,
+                cudaStream_t st) {
+    note_launch();
+    add_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(acc, x, c.d_mods, mm, c.N);
+}
+
+// ----------------------------------------------------------------------------
+// rescale (DivRoundByLastModulus)
+// ----------------------------------------------------------------------------
+__global__ void rescale_spread_kernel(const uint64_t *xL, long long xls, int L, uint64_t *t,
+                                      long long ts, const DevModulus *mods, int N) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int i = blockIdx.y, p = blockIdx.z;
+    const DevModulus mL = mods[L];
+    const uint64_t h = (mL.q - 1) >> 1;
+    uint64_t u = xL[(long long)p * xls + x] + h;
+    u = u >= mL.q ? u - mL.q : u;
+    const DevModulus m = mods[i];
+    const uint64_t ui = mred(u, m.mont1, m.q, m.qinv);
+    const uint64_t hi = mred(h, m.mont1, m.q, m.qinv);
+    t[(long long)p * ts + (long long)i * N + x] = sub_mod(ui, hi, m.q);
+}
+
+void launch_rescale_spread(const Context &c, const uint64_t *xL, long long xl_pstride, int L,
+                           uint64_t *t, long long t_pstride, int npolys, cudaStream_t st) {
+    note_launch();
+    rescale_spread_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(xL, xl_pstride, L, t,
+                                                                      t_pstride, c.d_mods, c.N);
+}
+
+__global__ void rescale_combine_kernel(const uint64_t *in, long long ins, const uint64_t *t,
+                                       long long ts, const uint64_t *rs, int L, uint64_t *out,
+                                       long long os, const DevModulus *mods, int N, int nQ) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int i = blockIdx.y, p = blockIdx.z;
+    const DevModulus m = mods[i];
+    const uint64_t a = in[(long long)p * ins + (long long)i * N + x];
+    const uint64_t tv = t[(long long)p * ts + (long long)i * N + x];
+    out[(long long)p * os + (long long)i * N + x] =
+        mred(tv + 2 * m.q - a, rs[(size_t)L * nQ + i], m.q, m.qinv);
+}
+
+void launch_rescale_combine(const Context &c, const uint64_t *in, long long in_pstride,
+                            const uint64_t *t, long long t_pstride, int L, uint64_t *out,
+                            long long out_pstride, int npolys, cudaStream_t st) {
+    note_launch();
+    rescale_combine_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(
+        in, in_pstride, t, t_pstride, c.d_rescale, L, out, out_pstride, c.d_mods, c.N, c.nQ);
+}
+
+__global__ void replicate_kernel(const uint64_t *src, uint64_t *dst, long long words, int ncopies,
+                                 long long ds) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= words) return;
+    const uint64_t v = src[i];
+    for (int c = 0; c < ncopies; ++c) dst[(long long)c * ds + i] = v;
+}
+
+void launch_replicate(const uint64_t *src, uint64_t *dst, long long words, int ncopies,
+                      long long dst_stride, cudaStream_t st) {
+    if (words <= 0 || ncopies <= 0) return;
+    note_launch();
+    replicate_kernel<<<(unsigned)((words + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+        src, dst, words, ncopies, dst_stride);
+}
+
+} // namespace mkf

@@ -1,0 +1,112 @@
+// Launchers for the non-NTT kernels of the mult+relin path.
+#pragma once
+
+#include "context.h"
+
+namespace mkf {
+
+constexpr int kMaxParties = 64;
+
+// limb -> global modulus index: l < nq -> q_first + l, else p_first + (l - nq)
+struct ModMap {
+    int nq, q_first, p_first;
+    __host__ __device__ int operator()(int l) const { return l < nq ? q_first + l : p_first + (l - nq); }
+};
+inline ModMap qmap(int n) { return ModMap{n, 0, 0}; }
+
+// Gadget decomposition (ModUp) of `npolys` polynomials into digits
+// [digit0, digit0+ndigits), coefficient domain in and out, canonical output.
+// `in` holds the ring's limbs (Q, or R = Q|QMul when ring_r) in the
+// coefficient domain; `level` is the Q level.  Output digit layout:
+// [level+1 Q limbs][nP P limbs].  Reference: software/kklss/mkrlwe/
+// basis_extension.go:428-535 (raw-copy branch included).
+void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
+                      int level, int gamma, int digit0, int ndigits, uint64_t *out,
+                      long long out_dstride, long long out_pstride, int npolys, cudaStream_t st);
+
+// Inner products of digit polynomials with key polynomials (Montgomery: B in
+// MForm):
+//   out[g][i][o][l] (+)= sum_t A[g][i][t][l] (.) B[g][t][o][l]
+// for groups g, inputs i < nin, outputs o < nout, limbs l < L1 + nP, terms t.
+// Limb l of A/out is at l*N; limb l of B is at l*N for l < L1 and at
+// (b_qlimbs + l - L1)*N for P limbs (full-level keys: b_qlimbs = nQ).
+struct IpArgs {
+    const uint64_t *A = nullptr;
+    long long a_tstride = 0, a_gstride = 0, a_istride = 0;
+    const uint64_t *B = nullptr;
+    long long b_tstride = 0, b_ostride = 0, b_gstride = 0;
+    int b_qlimbs = 0;
+    uint64_t *out = nullptr;
+    long long out_ostride = 0, out_gstride = 0, out_istride = 0;
+    int nterms = 0, nin = 1, nout = 1, groups = 1;
+    int L1 = 0, nP = 0;
+    int mform_out = 0, accumulate = 0;
+    // optional per-group (or, with bptr_per_term, per-term) B base pointers,
+    // passed by value so that no table has to be uploaded per call
+    int use_bptr = 0, bptr_per_term = 0;
+    const uint64_t *bptr[kMaxParties] = {};
+};
+void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st);
+
+// Exact basis extension (modUpExact, basis_extension.go:337-357) of npolys
+// polynomials: tab.ns source limbs at src (+p*src_pstride, limb i at i*N) to
+// the table rows [row0, row0+nt) written at out (+p*out_pstride, limb j at
+// j*N), target moduli tgt(j).  canonical = 0 keeps multSum's exact lazy
+// representative (the reference copies it raw into other moduli).
+void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, long long src_pstride,
+                  uint64_t *out, long long out_pstride, int row0, int nt, ModMap tgt, int canonical,
+                  int npolys, cudaStream_t st);
+
+// ModDown combine (basis_extension.go:203-229): r = MRed(y + 2q - x, negc[l])
+// = (x - y) * C^-1 over nl limbs of npolys polynomials (x == nullptr: x = 0).
+// r is summed over `terms` (x, y at +t*x_tstride / +t*y_tstride) before
+// being stored; accumulate adds into out.
+struct CombineSpec {
+    const uint64_t *x = nullptr;
+    long long x_pstride = 0, x_tstride = 0;
+    const uint64_t *y = nullptr;
+    long long y_pstride = 0, y_tstride = 0;
+    int terms = 1;
+    const uint64_t *negc = nullptr;
+    uint64_t *out = nullptr;
+    long long out_pstride = 0;
+    int accumulate = 0;
+};
+void launch_moddown_combine(const Context &c, const CombineSpec &s, int nl, ModMap mm, int npolys,
+                            cudaStream_t st);
+
+// Karatsuba tensor over nl limbs: mu0 = a0 b0, mu2 = a1 b1,
+// mu1 = (a0 + a1)(b0 + b1) - mu0 - mu2 (software/mkf/mkf_cpu/ckks.go:120-131).
+void launch_karatsuba(const Context &c, const uint64_t *a0, const uint64_t *a1, const uint64_t *b0,
+                      const uint64_t *b1, uint64_t *mu0, uint64_t *mu1, uint64_t *mu2, int nl,
+                      ModMap mm, cudaStream_t st);
+
+// KKLSS direct tensor (mkrlwe/keyswitch_hoisted.go:469-491 and the R-basis
+// form mkbfv/keyswitch_hoisted.go:154-200): c0 = a0 b0,
+// c_j = b0 a_j [has0_j] + a0 b_j [has1_j]; a, b, c are [k+1][nl][N].
+void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out,
+                         const unsigned char *d_has0, const unsigned char *d_has1, int k, int nl,
+                         ModMap mm, long long comp_stride, cudaStream_t st);
+
+// out = x * const (const per limb, stored in MForm), npolys polys.
+void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
+                      const uint64_t *mform_const, uint64_t *out, long long out_pstride, int nl,
+                      ModMap mm, int npolys, cudaStream_t st);
+// acc += x
+void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModMap mm,
+                cudaStream_t st);
+
+// Rescale by q_L (rounded, DivRoundByLastModulus): spread builds, for every
+// i < L, t_i = ([x_L + h]_{q_L} - h) mod q_i from the coefficient-domain last
+// limb; combine (after an optional NTT of t) gives out_i = (in_i - t_i)/q_L.
+void launch_rescale_spread(const Context &c, const uint64_t *xL, long long xl_pstride, int L,
+                           uint64_t *t, long long t_pstride, int npolys, cudaStream_t st);
+void launch_rescale_combine(const Context &c, const uint64_t *in, long long in_pstride,
+                            const uint64_t *t, long long t_pstride, int L, uint64_t *out,
+                            long long out_pstride, int npolys, cudaStream_t st);
+
+// Replicate `words` words of src into ncopies destinations.
+void launch_replicate(const uint64_t *src, uint64_t *dst, long long words, int ncopies,
+                      long long dst_stride, cudaStream_t st);
+
+} // namespace mkf
