@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-key mult+relin path on B200.
+
+Workload (one "product" = one MKF-CKKS mult+relin+rescale+materialize, the
+timed region of CKKSCase.Run, software/mkf/mkf_cpu/ckks.go:241-292):
+logN=16, k=8 parties, Q = one 60-bit + twenty-three 50-bit primes, P = four
+60-bit primes, scale 2^50, top level (24 limbs), operands in the NTT domain.
+Synthetic data: uniformly random key and ciphertext words (the keys of the
+reference are pseudo-random; their values do not change the work).
+
+A step = `--batch` products.  `value` is the batched form (the products of a
+step spread over `--streams` CUDA streams, each with its own workspace);
+`plain` is one product at a time on one stream.  Latency percentiles are the
+plain per-product device times.  Inputs (1.6 GB of keys) exceed the 126 MB L2.
+
+`--impl reference` times the reference algorithm's CPU restatement (the
+oracle; the reference's Go + Lattigo v2.3.0 is not installable here) on all
+host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mult+relin ops/s at logN=16,k=8: batched/served vs plain GPU; p50/p99 latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mkf_b200", choices=["mkf_b200", "reference"])
+    ap.add_argument("--config", default="C3")
+    ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--level", type=int, default=-1)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle: test infrastructure, timed here as the baseline)
+# ---------------------------------------------------------------------------
+def _cpu_product_worker(args):
+    config, k, level, what, seed = args
+    sys.path.insert(0, ROOT)
+    from mkf_b200 import params
+    from oracle.oracle import Oracle
+    from oracle import keygen as kg
+    lit = params.get("ckks", config)
+    o = Oracle.from_literal(lit)
+    N = o.n
+    nQ, nP = len(lit.q), len(lit.p)
+    beta = (nQ + nP - 1) // nP
+    g = kg.rng(seed)
+    L1 = level + 1
+    key = np.stack([np.stack([np.concatenate([kg.uniform(g, lit.q, N), kg.uniform(g, lit.p, N)])
+                              for _ in range(2)]) for _ in range(beta)])
+    if what == "switch":
+        x = kg.uniform(g, lit.q[:L1], N)
+        t0 = time.perf_counter()
+        o.mkf_switch_one(level, x, key, True, True)
+        return time.perf_counter() - t0
+    if what == "rescale":
+        x = kg.uniform(g, lit.q[:L1], N)
+        t0 = time.perf_counter()
+        o.rescale(level, x, True)
+        o.rescale(level, x, True)
+        return time.perf_counter() - t0
+    # full product
+    fold = np.stack([key] * k)
+    left = np.stack([kg.uniform(g, lit.q[:L1], N) for _ in range(k + 1)])
+    right = np.stack([kg.uniform(g, lit.q[:L1], N) for _ in range(k + 1)])
+    t0 = time.perf_counter()
+    o.mkf_ckks_mulrelin(k, level, left, right, fold, key, True, lit.scale, lit.scale ** 2)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(config, k, level):
+    """One full product on one core (about 15-25 s of CPU work)."""
+    t = _cpu_product_worker((config, k, level, "product", 7))
+    return {"value": 1.0 / t, "unit": "mult+relin ops/s", "cores": 1, "kind": "port",
+            "sample": f"one full MKF-CKKS mult+relin+rescale ({config}, k={k}, level {level}) "
+                      f"by the C oracle on one core: {t:.2f} s"}
+
+
+def run_reference(a):
+    """--impl reference: the CPU restatement on every host core."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from mkf_b200 import params
+    lit = params.get("ckks", a.config)
+    level = lit.max_level if a.level < 0 else a.level
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        # per-product overhead beyond the 2k+1 switches, timed once
+        t_resc = pool.map(_cpu_product_worker, [(a.config, a.k, level, "rescale", 1)])[0]
+        for _ in range(max(1, a.warmup)):
+            pool.map(_cpu_product_worker, [(a.config, a.k, level, "switch", 10 + i) for i in range(cores)])
+        times = []
+        for s in range(a.steps):
+            # the workers run concurrently; a step lasts as long as its slowest switch
+            r = pool.map(_cpu_product_worker, [(a.config, a.k, level, "switch", 100 + s * cores + i)
+                                               for i in range(cores)])
+            times.append(max(r))
+    t_step = sum(times) / len(times)
+    switches = 2 * a.k + 1
+    t_product = switches * t_step + t_resc  # wall time of `cores` products done in parallel
+    value = cores / t_product
+    sample = (f"each step: one MKF switchOne per worker on {cores} worker processes "
+              f"({a.config}, level {level}); a product = {switches} switches + a 2-poly rescale "
+              f"({t_resc:.2f} s, timed once)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "mult+relin ops/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"MKF-CKKS mult+relin+rescale {a.config} logN=16 k={a.k} "
+                                   f"level {level}", "parties": a.k, "level": level},
+            "cpu_baseline": {"value": value, "unit": "mult+relin ops/s", "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "mult+relin ops/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "Go and Lattigo v2.3.0 are absent on this box; the reference algorithm is "
+                    "timed through its C restatement (oracle/)."}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+def random_limbs(g, moduli, n, count=1):
+    out = np.empty((count, len(moduli), n), np.uint64)
+    for c in range(count):
+        for i, q in enumerate(moduli):
+            out[c, i] = g.integers(0, int(q), size=n, dtype=np.uint64)
+    return out
+
+
+def run_gpu(a):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from mkf_b200 import capi, params
+    from mkf_b200 import evaluator as ev
+
+    lit = params.get("ckks", a.config)
+    level = lit.max_level if a.level < 0 else a.level
+    k = a.k
+    N = lit.n
+    P = ev.Parameters(lit, "ckks", device=local)
+    g = np.random.Generator(np.random.PCG64(1234 + rank))
+    nQ, nP = len(lit.q), len(lit.p)
+    beta = (nQ + nP - 1) // nP
+    qp = list(lit.q) + list(lit.p)
+
+    def key():
+        return np.ascontiguousarray(random_limbs(g, qp, N, 2 * beta).reshape(beta, 2, nQ + nP, N))
+
+    ks = ev.MKFKeySet(P, [key() for _ in range(k)], key())
+    E = ev.MKFEvaluator(P, ks)
+    L1 = level + 1
+    nin = max(a.batch, 1)
+    ins = []
+    for _ in range(nin):
+        l = ev.Ciphertext.from_array(P, random_limbs(g, lit.q[:L1], N, k + 1), True, scale=lit.scale)
+        r = ev.Ciphertext.from_array(P, random_limbs(g, lit.q[:L1], N, k + 1), True, scale=lit.scale)
+        ins.append((l, r))
+    lout = E.output_level(ins[0][0], ins[0][1], True)
+    outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(nin)]
+    streams = [torch.cuda.Stream() for _ in range(max(1, a.streams))]
+
+    def product(i, s):
+        l, r = ins[i % nin]
+        E.MulRelin(l, r, outs[i % nin], rescale=True, materialize=True,
+                   stream=ctypes_stream(s))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- plain: one product at a time on one stream -------------------------
+    L = capi.lib()
+    s0 = streams[0]
+    for i in range(a.warmup):
+        product(i, s0)
+    barrier()
+    L.mkf_profile_enable(P.handle, 1)
+    lat = []
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    plain_steps = max(a.steps, 5)
+    t_plain = 0.0
+    for i in range(plain_steps):
+        ev0.record(s0)
+        product(i, s0)
+        ev1.record(s0)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        lat.append(ms)
+        t_plain += ms
+    barrier()
+    plain_ops = ws * plain_steps / (max_over_ranks(t_plain) / 1e3)
+    nk = L.mkf_profile_kinds()
+    pms = (ctypes.c_double * nk)()
+    pcnt = (ctypes.c_uint64 * nk)()
+    pby = (ctypes.c_double * nk)()
+    L.mkf_profile_read(P.handle, pms, pcnt, pby)
+    L.mkf_profile_enable(P.handle, 0)
+
+    # ---- batched: `batch` products per step over `streams` streams -------------
+    def batched_step(step):
+        start = torch.cuda.Event()
+        start.record(streams[0])
+        for s in streams[1:]:
+            s.wait_event(start)
+        for j in range(a.batch):
+            product(step * a.batch + j, streams[j % len(streams)])
+        for s in streams[1:]:
+            e = torch.cuda.Event()
+            e.record(s)
+            streams[0].wait_event(e)
+
+    for i in range(a.warmup):
+        batched_step(i)
+    barrier()
+    L.mkf_launch_count(1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(streams[0])
+    for step in range(a.steps):
+        batched_step(step)
+    t1.record(streams[0])
+    t1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = int(L.mkf_launch_count(0))
+    total_ms = max_over_ranks(t0.elapsed_time(t1))
+    value = ws * a.steps * a.batch / (total_ms / 1e3)
+
+    kinds = {}
+    for i in range(nk):
+        nm = L.mkf_profile_kind_name(i).decode()
+        if pcnt[i]:
+            kinds[nm] = {"ms": pms[i], "launches": int(pcnt[i]), "bytes": pby[i]}
+    top = max(kinds.items(), key=lambda kv: kv[1]["ms"])
+    peak, peak_kind = measured_peaks()
+    tk = top[1]
+    avg_ms = tk["ms"] / tk["launches"]
+    bytes_per_launch = tk["bytes"] / tk["launches"]
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
+                "share": tk["ms"] / sum(v["ms"] for v in kinds.values()),
+                "timed_in": "plain region (one stream, no overlap)"}
+
+    # ---- e2e through the C ABI with pinned host buffers -------------------------
+    e2e = None
+    if not a.no_e2e:
+        words_in = (k + 1) * L1 * N
+        words_out = (k + 1) * (lout + 1) * N
+        hin = [torch.empty(words_in, dtype=torch.int64, pin_memory=True) for _ in range(2 * a.batch)]
+        for h in hin:
+            h.numpy().view(np.uint64)[:] = g.integers(0, int(lit.q[-1]), size=words_in, dtype=np.uint64)
+        hout = [torch.empty(words_out, dtype=torch.int64, pin_memory=True) for _ in range(a.batch)]
+        e_ins = [(ev.Ciphertext(P, k + 1, level, True, scale=lit.scale),
+                  ev.Ciphertext(P, k + 1, level, True, scale=lit.scale)) for _ in range(a.batch)]
+        e_outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.batch)]
+
+        def e2e_step():
+            start = torch.cuda.Event()
+            start.record(streams[0])
+            for s in streams[1:]:
+                s.wait_event(start)
+            for j in range(a.batch):
+                s = streams[j % len(streams)]
+                cs = ctypes_stream(s)
+                l, r = e_ins[j]
+                capi.check(P.handle, L.mkf_ct_upload_async(
+                    l.handle, ctypes.cast(hin[2 * j].data_ptr(), capi.u64p), words_in, cs))
+                capi.check(P.handle, L.mkf_ct_upload_async(
+                    r.handle, ctypes.cast(hin[2 * j + 1].data_ptr(), capi.u64p), words_in, cs))
+                E.MulRelin(l, r, e_outs[j], rescale=True, materialize=True, stream=cs)
+                capi.check(P.handle, L.mkf_ct_download_async(
+                    e_outs[j].handle, ctypes.cast(hout[j].data_ptr(), capi.u64p), words_out, cs))
+            for s in streams[1:]:
+                e = torch.cuda.Event()
+                e.record(s)
+                streams[0].wait_event(e)
+
+        for _ in range(a.warmup):
+            e2e_step()
+        barrier()
+        t0.record(streams[0])
+        for _ in range(a.steps):
+            e2e_step()
+        t1.record(streams[0])
+        t1.synchronize()
+        barrier()
+        e_ms = max_over_ranks(t0.elapsed_time(t1))
+        e2e = {"value": ws * a.steps * a.batch / (e_ms / 1e3), "unit": "mult+relin ops/s",
+               "h2d_bytes_per_step": 2 * a.batch * words_in * 8,
+               "d2h_bytes_per_step": a.batch * words_out * 8}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a.config, k, level)
+
+    if rank == 0:
+        lat_sorted = sorted(lat)
+        line = {
+            "metric": METRIC, "value": value, "unit": "mult+relin ops/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (uniform random key and ciphertext words)",
+            "config": {"workload": f"MKF-CKKS mult+relin+rescale+materialize {a.config}: logN=16, "
+                                   f"k={k}, Q=1x60b+23x50b, P=4x60b, level {level}",
+                       "parties": k, "level": level, "batch_per_step": a.batch,
+                       "streams": len(streams), "l2": "inputs (keys 1.6 GB) larger than L2",
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "plain": {"value": plain_ops, "unit": "mult+relin ops/s"},
+            "batched_over_plain": value / plain_ops,
+            "latency_ms": {"p50": lat_sorted[len(lat) // 2],
+                           "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "kernels": kinds,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+import ctypes  # noqa: E402
+
+
+def ctypes_stream(s):
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_gpu(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -193,6 +193,15 @@ mkf_status mkf_switch_one_host(mkf_ctx *ctx, int level, int in_ntt, const uint64
                                const uint64_t *key, int ntt_output, uint64_t *out0,
                                uint64_t *out1);
 
+/* Per-kernel-kind CUDA-event timing (the reference's stage profiler,
+ * software/kklss/stageprof/stageprof.go).  enable=1 clears and starts
+ * recording; read fills ms/launches/algorithmic bytes per kind
+ * (arrays of mkf_profile_kinds() entries) and synchronizes. */
+mkf_status mkf_profile_enable(mkf_ctx *ctx, int enable);
+int mkf_profile_kinds(void);
+const char *mkf_profile_kind_name(int kind);
+mkf_status mkf_profile_read(mkf_ctx *ctx, double *ms, uint64_t *launches, double *bytes);
+
 /* Number of this library's kernels launched on the calling thread since the
  * last reset (instrumentation for the benchmark). */
 uint64_t mkf_launch_count(int reset);

@@ -105,6 +105,11 @@ def lib():
         "mkf_ntt_host": (i, [vp, i, i, i, u64p, u64p, i]),
         "mkf_decompose_host": (i, [vp, i, i, u64p, u64p]),
         "mkf_switch_one_host": (i, [vp, i, i, u64p, u64p, i, u64p, u64p]),
+        "mkf_profile_enable": (i, [vp, i]),
+        "mkf_profile_kinds": (i, []),
+        "mkf_profile_kind_name": (ctypes.c_char_p, [i]),
+        "mkf_profile_read": (i, [vp, ctypes.POINTER(d), ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.POINTER(d)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -132,6 +132,28 @@ uint64_t mkf_launch_count(int reset) {
     return g_launches.load();
 }
 
+mkf_status mkf_profile_enable(mkf_ctx *ctx, int enable) {
+    if (!ctx) return MKF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->c.device);
+    cudaDeviceSynchronize();
+    ctx->c.prof.reset();
+    ctx->c.prof.on = enable != 0;
+    return MKF_OK;
+}
+
+int mkf_profile_kinds(void) { return PK_COUNT; }
+
+const char *mkf_profile_kind_name(int kind) {
+    return kind >= 0 && kind < PK_COUNT ? kProfNames[kind] : "";
+}
+
+mkf_status mkf_profile_read(mkf_ctx *ctx, double *ms, uint64_t *launches, double *bytes) {
+    if (!ctx || !ms || !launches || !bytes) return MKF_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->c.device);
+    ctx->c.prof.read(ms, launches, bytes);
+    return cuda_check(ctx, "profile");
+}
+
 mkf_status mkf_ctx_create(const mkf_params_desc *d, mkf_ctx **out) {
     if (!d || !out) return MKF_ERR_INVALID_ARG;
     *out = nullptr;

@@ -134,6 +134,56 @@ static uint64_t bitrev(uint64_t x, int bits) {
     return r;
 }
 
+const char *const kProfNames[PK_COUNT] = {
+    "ntt_fwd_col", "ntt_fwd_row", "ntt_fwd_full", "ntt_inv_row", "ntt_inv_col", "ntt_inv_full",
+    "decompose", "keyswitch_ip", "modup", "moddown_combine", "tensor", "rescale", "elementwise"};
+
+int Profiler::begin(int kind, cudaStream_t st, double bytes) {
+    std::lock_guard<std::mutex> g(mu);
+    if (used == recs.size()) {
+        Rec r{};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        recs.push_back(r);
+    }
+    Rec &r = recs[used];
+    r.kind = kind;
+    r.bytes = bytes;
+    cudaEventRecord(r.a, st);
+    return (int)used++;
+}
+
+void Profiler::end(int idx, cudaStream_t st) { cudaEventRecord(recs[idx].b, st); }
+
+void Profiler::reset() {
+    std::lock_guard<std::mutex> g(mu);
+    used = 0;
+}
+
+void Profiler::read(double *ms, uint64_t *count, double *bytes) {
+    std::lock_guard<std::mutex> g(mu);
+    for (int k = 0; k < PK_COUNT; ++k) {
+        ms[k] = 0;
+        count[k] = 0;
+        bytes[k] = 0;
+    }
+    for (size_t i = 0; i < used; ++i) {
+        float t = 0;
+        cudaEventSynchronize(recs[i].b);
+        cudaEventElapsedTime(&t, recs[i].a, recs[i].b);
+        ms[recs[i].kind] += t;
+        count[recs[i].kind] += 1;
+        bytes[recs[i].kind] += recs[i].bytes;
+    }
+}
+
+Profiler::~Profiler() {
+    for (auto &r : recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+}
+
 Context::~Context() {
     int prev = 0;
     cudaGetDevice(&prev);
@@ -196,7 +246,7 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
     scale = scale_;
     t = t_;
     device = device_;
-    if (logN < 4 || logN > 17) return "logN out of range [4,17]";
+    if (logN < 4 || logN > 16) return "logN out of range [4,16]";
     if (nQ < 1 || nQ > 60 || nP < 1 || nP > 16 || nQM < 0 || nQM > 60)
         return "modulus counts out of range";
     Q.assign(q, q + nq);
@@ -223,8 +273,8 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         n1 = logN;
         n2 = 0;
     } else {
-        n2 = 8;
-        n1 = logN - 8;
+        n2 = (logN + 1) / 2; // row stages (contiguous rows of 2^n2 words)
+        n1 = logN - n2;      // column stages
     }
     const int S1 = 1 << n1;
 

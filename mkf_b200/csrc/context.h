@@ -23,6 +23,33 @@ struct ModUpTab {
     const uint64_t *vq = nullptr;    // [nt][ns+1] v*(p_j - Q mod p_j) mod p_j
 };
 
+// Per-kernel-kind CUDA-event timing (the reference's exclusive stage timers,
+// software/kklss/stageprof/stageprof.go, mapped onto this library's kernels).
+enum ProfKind : int {
+    PK_NTT_FWD_COL, PK_NTT_FWD_ROW, PK_NTT_FWD_FULL, PK_NTT_INV_ROW, PK_NTT_INV_COL,
+    PK_NTT_INV_FULL, PK_DECOMPOSE, PK_IP, PK_MODUP, PK_COMBINE, PK_TENSOR, PK_RESCALE,
+    PK_ELEMENTWISE, PK_COUNT
+};
+extern const char *const kProfNames[PK_COUNT];
+
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Rec> recs;
+    size_t used = 0;
+    std::mutex mu;
+    int begin(int kind, cudaStream_t st, double bytes);
+    void end(int idx, cudaStream_t st);
+    void reset();
+    // totals per kind (synchronizes the recorded events)
+    void read(double *ms, uint64_t *count, double *bytes);
+    ~Profiler();
+};
+
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -77,6 +104,7 @@ class Context {
 
     std::string last_error;
     std::mutex err_mu;
+    mutable Profiler prof;
 
     void set_error(const std::string &s) {
         std::lock_guard<std::mutex> g(err_mu);
@@ -108,5 +136,18 @@ uint64_t h_mform(uint64_t a, uint64_t q);
 uint64_t h_shoup(uint64_t w, uint64_t q);
 uint64_t h_primitive_root(uint64_t q);
 bool h_is_prime(uint64_t n);
+
+// RAII timing scope around one kernel launch (no-op unless profiling).
+struct ProfScope {
+    const Context &c;
+    int idx = -1;
+    cudaStream_t st;
+    ProfScope(const Context &ctx, int kind, cudaStream_t s, double bytes) : c(ctx), st(s) {
+        if (c.prof.on) idx = c.prof.begin(kind, st, bytes);
+    }
+    ~ProfScope() {
+        if (idx >= 0) c.prof.end(idx, st);
+    }
+};
 
 } // namespace mkf

@@ -146,6 +146,7 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     uint64_t *yq = bfv ? ar.take(3 * poly) : nullptr;
     uint64_t *last = bfv ? nullptr : ar.take(2LL * N);
     uint64_t *tr = bfv ? nullptr : ar.take(2 * poly);
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, 2 * k));
     if (ar.dry) return "";
 
     // 1. gadget decomposition of every component of both operands
@@ -153,14 +154,12 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         d2d2(coeff, poly, left.data + left.cs, left.cs, poly, k, st);
         d2d2(coeff + kk * poly, poly, right.data + right.cs, right.cs, poly, k, st);
         ntt_inverse(c, lsq(coeff, poly, L1), 2 * k, st);
-        launch_decompose(c, coeff, poly, 0, level, 1, 0, beta, dig, qp, beta * qp, 2 * k, st);
+        decompose_ntt(c, coeff, poly, 0, level, 1, beta, dig, 2 * k, dscr, st);
     } else {
-        launch_decompose(c, left.data + left.cs, left.cs, 0, level, 1, 0, beta, dig, qp, beta * qp,
-                         k, st);
-        launch_decompose(c, right.data + right.cs, right.cs, 0, level, 1, 0, beta,
-                         dig + kk * beta * qp, qp, beta * qp, k, st);
+        decompose_ntt(c, left.data + left.cs, left.cs, 0, level, 1, beta, dig, k, dscr, st);
+        decompose_ntt(c, right.data + right.cs, right.cs, 0, level, 1, beta, dig + kk * beta * qp, k,
+                      dscr, st);
     }
-    ntt_forward(c, lsqp(c, dig, qp, L1), 2 * k * beta, st);
 
     // 2. fold key inner products: each key read once for both operands
     IpArgs ip;
@@ -242,8 +241,7 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         }
     }
     // relinearization key switch of mu2 (coefficient domain input)
-    launch_decompose(c, bfv ? mu2 : rcoef, poly, 0, level, 1, 0, beta, rdig, qp, beta * qp, 1, st);
-    ntt_forward(c, lsqp(c, rdig, qp, L1), beta, st);
+    decompose_ntt(c, bfv ? mu2 : rcoef, poly, 0, level, 1, beta, rdig, 1, dscr, st);
     {
         IpArgs r;
         r.A = rdig;
@@ -332,6 +330,7 @@ std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int sch
     uint64_t *ym = bfv ? ar.take(K1 * (long long)c.nQM * N) : nullptr;
     uint64_t *trs = bfv ? nullptr : ar.take(K1 * poly);
     uint8_t *ones = reinterpret_cast<uint8_t *>(ar.take(kMaxParties / 8 + 1));
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, nd, k));
     if (ar.dry) return "";
     fill_ones(ones, k, st);
 
@@ -366,9 +365,8 @@ std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int sch
         d1 = BR + rp;
         d1s = rp;
     }
-    launch_decompose(c, d0, d0s, bfv, level, 2, 0, nd, H0, qp, nd * qp, k, st);
-    launch_decompose(c, d1, d1s, bfv, level, 2, 0, nd, H1, qp, nd * qp, k, st);
-    ntt_forward(c, lsqp(c, H0, qp, L1), 2 * k * nd, st); // H0 and H1 are adjacent
+    decompose_ntt(c, d0, d0s, bfv, level, 2, nd, H0, k, dscr, st);
+    decompose_ntt(c, d1, d1s, bfv, level, 2, nd, H1, k, dscr, st);
 
     // 2. x = MForm(sum_i d_i (.) g(op0_i)), y = MForm(sum_j b_j (.) g(op1_j))
     //    (mkrlwe/keyswitch_hoisted.go:84-123; mkbfv/keyswitch_hoisted.go:100-148)
@@ -445,8 +443,7 @@ std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int sch
     launch_ip(c, ext, st);
     moddown_prepare(c, st, E, qp, k, L1, 0, tmp);
     launch_moddown_combine(c, pdown(c, E, qp, tmp, poly, Tq, poly, 0), L1, qmap(L1), k, st);
-    launch_decompose(c, Tq, poly, 0, level, 2, 0, beta, G, qp, beta * qp, k, st);
-    ntt_forward(c, lsqp(c, G, qp, L1), k * beta, st);
+    decompose_ntt(c, Tq, poly, 0, level, 2, beta, G, k, dscr, st);
     {
         IpArgs v;
         v.A = G;
@@ -508,11 +505,11 @@ std::string switch_one(const Context &c, Arena &ar, cudaStream_t st, int level, 
     uint64_t *dig = ar.take(beta * qp);
     uint64_t *acc = ar.take(2 * qp);
     uint64_t *tmp = ar.take(2 * poly);
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, 1));
     if (ar.dry) return "";
     d2d2(coeff, poly, in, poly, poly, 1, st);
     if (in_ntt) ntt_inverse(c, lsq(coeff, poly, L1), 1, st);
-    launch_decompose(c, coeff, poly, 0, level, 1, 0, beta, dig, qp, beta * qp, 1, st);
-    ntt_forward(c, lsqp(c, dig, qp, L1), beta, st);
+    decompose_ntt(c, coeff, poly, 0, level, 1, beta, dig, 1, dscr, st);
     IpArgs r;
     r.A = dig;
     r.a_tstride = qp;
@@ -570,10 +567,9 @@ std::string decompose_poly(const Context &c, Arena &ar, cudaStream_t st, int gam
     if (c.nP % gamma) return "gamma must divide the number of special primes";
     if (c.nP / gamma > 8) return "at most 8 limbs per digit are supported";
     const int beta = c.beta_of(level, gamma);
-    const long long qp = (long long)(level + 1 + c.nP) * c.N;
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, gamma, beta, 1));
     if (ar.dry) return "";
-    launch_decompose(c, in_coeff, 0, 0, level, gamma, 0, beta, out, qp, beta * qp, 1, st);
-    ntt_forward(c, lsqp(c, out, qp, level + 1), beta, st);
+    decompose_ntt(c, in_coeff, 0, 0, level, gamma, beta, out, 1, dscr, st);
     return "";
 }
 

@@ -4,6 +4,8 @@
 // kernels: one thread per coefficient, coalesced 8-byte accesses along the
 // coefficient axis, limbs / digits / polynomials on the other grid axes.
 #include "kernels.h"
+#include "modup.cuh"
+#include "ntt.h"
 
 #include <algorithm>
 
@@ -13,56 +15,6 @@ constexpr int kBlock = 256;
 
 static inline dim3 grid_for(int N, int y = 1, int z = 1) {
     return dim3((N + kBlock - 1) / kBlock, y, z);
-}
-
-// ----------------------------------------------------------------------------
-// exact basis extension pieces (software/kklss/mkrlwe/basis_extension.go)
-// ----------------------------------------------------------------------------
-
-// reconstructRNS (basis_extension.go:537-579): y_i = MRed(x_i, inv_i) and the
-// correction v = floor(sum_i y_i / q_i) in IEEE double, in the reference's
-// order, with explicit round-to-nearest intrinsics so that nothing is
-// reassociated or contracted.
-template <int MAXNS>
-MKF_DEV uint64_t reconstruct(const uint64_t *x, const ModUpTab &tab, const DevModulus *mods,
-                             uint64_t *y) {
-    double vi = 0.0;
-#pragma unroll
-    for (int i = 0; i < MAXNS; ++i) {
-        if (i < tab.ns) {
-            const DevModulus &m = mods[tab.src_mod[i]];
-            y[i] = mred(x[i], tab.inv[i], m.q, m.qinv);
-            vi = __dadd_rn(vi, __ddiv_rn(__ull2double_rn(y[i]), m.qd));
-        }
-    }
-    return __double2ull_rz(vi);
-}
-
-// multSum (basis_extension.go:581-646): sum y_i * qmod_i on 128 bits, lazy
-// Montgomery reduction, plus v*(-Q mod p).  Returns the exact representative
-// the reference produces.
-template <int MAXNS>
-MKF_DEV uint64_t multsum(const uint64_t *y, const ModUpTab &tab, int row, uint64_t v,
-                         const DevModulus &pm) {
-    const uint64_t *qm = tab.qmod + (size_t)row * tab.ns;
-    uint64_t lo = 0, hi = 0;
-#pragma unroll
-    for (int i = 0; i < MAXNS; ++i) {
-        if (i < tab.ns) {
-            const uint64_t b = qm[i];
-            const uint64_t pl = y[i] * b, ph = __umul64hi(y[i], b);
-            const uint64_t nl = lo + pl;
-            hi += ph + (nl < lo ? 1 : 0);
-            lo = nl;
-        }
-    }
-    const uint64_t h = __umul64hi(lo * pm.qinv, pm.q);
-    return hi - h + pm.q + tab.vq[(size_t)row * (tab.ns + 1) + v];
-}
-
-MKF_DEV uint64_t canon(uint64_t x, uint64_t q) {
-    while (x >= q) x -= q;
-    return x;
 }
 
 // ----------------------------------------------------------------------------
@@ -145,8 +97,78 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
     a.nP = c.nP;
     a.N = c.N;
     a.pmod0 = c.pidx(0);
+    ProfScope ps(c, PK_DECOMPOSE, st,
+                 8.0 * c.N * npolys * ndigits * (a.alpha + level + 1 + c.nP));
     note_launch();
     decompose_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(a);
+}
+
+// y_i and the float64 correction of every (poly, digit, coefficient)
+__global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in, long long in_pstride,
+                                                             const ModUpTab *tabs,
+                                                             const DevModulus *mods, uint64_t *y,
+                                                             uint8_t *v, int level, int alpha,
+                                                             int ndigits, int N) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int d = blockIdx.y, p = blockIdx.z;
+    const int ns = (level > alpha * (d + 1) - 1 ? alpha - 2 : (level % alpha) - 1) + 2;
+    if (ns < 2) return;
+    const ModUpTab tab = tabs[d * (alpha + 1) + ns];
+    const uint64_t *xp = in + (long long)p * in_pstride + (long long)d * alpha * N + x;
+    const long long pd = (long long)p * ndigits + d;
+    uint64_t *yp = y + pd * alpha * N + x;
+    double vi = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (i < ns) {
+            const DevModulus &m = mods[tab.src_mod[i]];
+            const uint64_t yi = mred(xp[(long long)i * N], tab.inv[i], m.q, m.qinv);
+            yp[(long long)i * N] = yi;
+            vi = __dadd_rn(vi, __ddiv_rn(__ull2double_rn(yi), m.qd));
+        }
+    }
+    v[pd * N + x] = (uint8_t)__double2ull_rz(vi);
+}
+
+size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys) {
+    const size_t n = (size_t)npolys * ndigits * c.N;
+    return n * c.alpha_of(gamma) + (n + 7) / 8 + 64;
+}
+
+void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
+                   int level, int gamma, int ndigits, uint64_t *out, int npolys,
+                   uint64_t *scratch, cudaStream_t st) {
+    if (ndigits <= 0 || npolys <= 0) return;
+    const int L1 = level + 1, limbs = L1 + c.nP;
+    const long long qp = (long long)limbs * c.N;
+    if (c.n2 == 0) {
+        launch_decompose(c, in, in_pstride, ring_r, level, gamma, 0, ndigits, out, qp,
+                         ndigits * qp, npolys, st);
+        ntt_forward(c, LimbSet{out, qp, limbs, L1, 0, c.pidx(0)}, npolys * ndigits, st);
+        return;
+    }
+    const int alpha = c.alpha_of(gamma);
+    const size_t n = (size_t)npolys * ndigits * c.N;
+    uint64_t *y = scratch;
+    uint8_t *v = reinterpret_cast<uint8_t *>(scratch + n * alpha);
+    if (!ring_r && alpha >= 2) {
+        ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
+        note_launch();
+        digits_prep_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(
+            in, in_pstride, c.d_decomp[gamma - 1], c.d_mods, y, v, level, alpha, ndigits, c.N);
+    }
+    DigitSrc src;
+    src.x = in;
+    src.x_pstride = in_pstride;
+    src.y = y;
+    src.v = v;
+    src.tabs = ring_r ? nullptr : c.d_decomp[gamma - 1];
+    src.ndigits = ndigits;
+    src.alpha = alpha;
+    src.level = level;
+    src.nQ = c.nQ;
+    ntt_forward_digits(c, src, out, npolys, st);
 }
 
 // ----------------------------------------------------------------------------
@@ -201,6 +223,13 @@ void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
     if (a.groups <= 0 || a.nterms < 0) return;
     dim3 grid = grid_for(c.N, a.L1 + a.nP, a.groups);
     const int pm = c.pidx(0);
+    // algorithmic bytes: every digit word and key word read once, outputs written once
+    const double lim = 8.0 * c.N * (a.L1 + a.nP);
+    const bool bshared = !a.use_bptr && a.b_gstride == 0;
+    const double bytes = lim * ((double)a.groups * a.nin * a.nterms +
+                                (bshared ? 1.0 : a.groups) * a.nterms * a.nout +
+                                (double)a.groups * a.nin * a.nout * (a.accumulate ? 2 : 1));
+    ProfScope ps(c, PK_IP, st, bytes);
     note_launch();
     if (a.nin == 1 && a.nout == 1)
         ip_kernel<1, 1><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
@@ -250,6 +279,7 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
                   int npolys, cudaStream_t st) {
     if (npolys <= 0) return;
     ModUpArgs a{tab, src, src_pstride, out, out_pstride, c.d_mods, tgt, row0, nt, c.N, canonical};
+    ProfScope ps(c, PK_MODUP, st, 8.0 * c.N * npolys * (tab.ns + nt));
     dim3 grid = grid_for(c.N, npolys);
     note_launch();
     if (tab.ns <= 4)
@@ -290,6 +320,8 @@ __global__ void __launch_bounds__(kBlock) moddown_combine_kernel(CombineSpec a, 
 void launch_moddown_combine(const Context &c, const CombineSpec &s, int nl, ModMap mm, int npolys,
                             cudaStream_t st) {
     if (npolys <= 0 || nl <= 0) return;
+    ProfScope ps(c, PK_COMBINE, st,
+                 8.0 * c.N * nl * npolys * ((s.x ? 2.0 : 1.0) * s.terms + 1 + (s.accumulate ? 1 : 0)));
     note_launch();
     moddown_combine_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(s, mm, c.d_mods, c.N);
 }
@@ -321,6 +353,7 @@ __global__ void karatsuba_kernel(const uint64_t *a0, const uint64_t *a1, const u
 void launch_karatsuba(const Context &c, const uint64_t *a0, const uint64_t *a1, const uint64_t *b0,
                       const uint64_t *b1, uint64_t *mu0, uint64_t *mu1, uint64_t *mu2, int nl,
                       ModMap mm, cudaStream_t st) {
+    ProfScope ps(c, PK_TENSOR, st, 8.0 * c.N * nl * 7);
     note_launch();
     karatsuba_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(a0, a1, b0, b1, mu0, mu1, mu2, c.d_mods,
                                                             mm, c.N);
@@ -349,6 +382,7 @@ __global__ void kklss_tensor_kernel(const uint64_t *a, const uint64_t *b, uint64
 void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out,
                          const unsigned char *d_has0, const unsigned char *d_has1, int k, int nl,
                          ModMap mm, long long comp_stride, cudaStream_t st) {
+    ProfScope ps(c, PK_TENSOR, st, 8.0 * c.N * nl * 3.0 * (k + 1));
     note_launch();
     kklss_tensor_kernel<<<grid_for(c.N, nl, k + 1), kBlock, 0, st>>>(a, b, out, d_has0, d_has1,
                                                                       c.d_mods, mm, c.N,
@@ -369,6 +403,7 @@ __global__ void mul_const_kernel(const uint64_t *x, long long xps, const uint64_
 void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
                       const uint64_t *mform_const, uint64_t *out, long long out_pstride, int nl,
                       ModMap mm, int npolys, cudaStream_t st) {
+    ProfScope ps(c, PK_ELEMENTWISE, st, 16.0 * c.N * nl * npolys);
     note_launch();
     mul_const_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(x, x_pstride, mform_const, out,
                                                                    out_pstride, c.d_mods, mm, c.N);
@@ -386,6 +421,7 @@ __global__ void add_kernel(uint64_t *acc, const uint64_t *x, const DevModulus *m
 
 void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModMap mm,
                 cudaStream_t st) {
+    ProfScope ps(c, PK_ELEMENTWISE, st, 24.0 * c.N * nl);
     note_launch();
     add_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(acc, x, c.d_mods, mm, c.N);
 }
@@ -410,6 +446,7 @@ __global__ void rescale_spread_kernel(const uint64_t *xL, long long xls, int L, 
 
 void launch_rescale_spread(const Context &c, const uint64_t *xL, long long xl_pstride, int L,
                            uint64_t *t, long long t_pstride, int npolys, cudaStream_t st) {
+    ProfScope ps(c, PK_RESCALE, st, 8.0 * c.N * npolys * (L + 1));
     note_launch();
     rescale_spread_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(xL, xl_pstride, L, t,
                                                                       t_pstride, c.d_mods, c.N);
@@ -431,6 +468,7 @@ __global__ void rescale_combine_kernel(const uint64_t *in, long long ins, const 
 void launch_rescale_combine(const Context &c, const uint64_t *in, long long in_pstride,
                             const uint64_t *t, long long t_pstride, int L, uint64_t *out,
                             long long out_pstride, int npolys, cudaStream_t st) {
+    ProfScope ps(c, PK_RESCALE, st, 24.0 * c.N * npolys * L);
     note_launch();
     rescale_combine_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(
         in, in_pstride, t, t_pstride, c.d_rescale, L, out, out_pstride, c.d_mods, c.N, c.nQ);

@@ -24,6 +24,17 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
                       int level, int gamma, int digit0, int ndigits, uint64_t *out,
                       long long out_dstride, long long out_pstride, int npolys, cudaStream_t st);
 
+// Gadget decomposition followed by the forward NTT of every digit:
+// out[poly][digit] = NTT(digit d of in[poly]), layout [level+1+nP][N] per
+// digit, digits contiguous.  For logN >= 13 the digits are never stored in
+// the coefficient domain: a pre-pass writes y_i and the float64 correction
+// and the NTT column pass reconstructs each limb on load.  scratch must hold
+// decompose_ntt_scratch_words() words.
+size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys);
+void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
+                   int level, int gamma, int ndigits, uint64_t *out, int npolys,
+                   uint64_t *scratch, cudaStream_t st);
+
 // Inner products of digit polynomials with key polynomials (Montgomery: B in
 // MForm):
 //   out[g][i][o][l] (+)= sum_t A[g][i][t][l] (.) B[g][t][o][l]

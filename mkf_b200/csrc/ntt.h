@@ -10,6 +10,19 @@ namespace mkf {
 // Forward / inverse negacyclic NTT of every limb of `npolys` polynomials
 // described by `ls`, in place.  Inputs canonical; outputs canonical.
 void ntt_forward(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
+
+// Source of the fused gadget-decomposition + NTT (logN >= 13).
+struct DigitSrc {
+    const uint64_t *x = nullptr;   // coefficient-domain source polynomials (ring limbs)
+    long long x_pstride = 0;
+    const uint64_t *y = nullptr;   // [poly][digit][alpha][N]: y_i = MRed(x_i, (Q/q_i)^-1)
+    const uint8_t *v = nullptr;    // [poly][digit][N]: float64 correction
+    const ModUpTab *tabs = nullptr; // [digit][alpha+1] (null when every digit is one limb)
+    int ndigits = 0, alpha = 0, level = 0, nQ = 0;
+};
+// NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load.
+void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
+                        cudaStream_t st);
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
 
 } // namespace mkf

@@ -80,7 +80,29 @@ def mkf_ckks_decode(case: MKFCase, out, lv, scale):
     return kg.CKKSEncoder(lit.log_n).decode(kg.crt_centered(ph, lit.q[: lv + 1]), scale)
 
 
-def mkf_bfv_case(lit, k, seed=5) -> MKFCase:
+def sparse_message(g, n, t, nnz=8):
+    m = np.zeros(n, dtype=np.int64)
+    m[g.choice(n, nnz, replace=False)] = g.integers(0, t, nnz)
+    return m
+
+
+def sparse_negacyclic_mod(a, b, t):
+    n = len(a)
+    out = [0] * n
+    ia = [i for i in range(n) if a[i]]
+    ib = [j for j in range(n) if b[j]]
+    for i in ia:
+        for j in ib:
+            k = i + j
+            v = int(a[i]) * int(b[j])
+            if k >= n:
+                out[k - n] -= v
+            else:
+                out[k] += v
+    return np.array([x % t for x in out], dtype=object)
+
+
+def mkf_bfv_case(lit, k, seed=5, sparse=False) -> MKFCase:
     o = Oracle.from_literal(lit)
     R = kg.RNS(o)
     N = o.n
@@ -89,7 +111,7 @@ def mkf_bfv_case(lit, k, seed=5) -> MKFCase:
     g = kg.rng(seed + 1)
     cts, sums = [], []
     for _ in range(2):
-        ms = [g.integers(0, lit.t, N) for _ in range(k)]
+        ms = [sparse_message(g, N, lit.t) if sparse else g.integers(0, lit.t, N) for _ in range(k)]
         sums.append(np.sum(ms, axis=0) % lit.t)
         C0 = np.zeros((nq, N), np.uint64)
         comps = []
@@ -99,7 +121,10 @@ def mkf_bfv_case(lit, k, seed=5) -> MKFCase:
             C0 = o.add(C0, o.intt(c0, "Q"))
             comps.append(o.intt(c1, "Q"))
         cts.append(np.ascontiguousarray(np.stack([C0] + comps)))
-    want = negacyclic_mod(sums[0], sums[1], lit.t) if N <= 4096 else None
+    if sparse:
+        want = sparse_negacyclic_mod(sums[0], sums[1], lit.t)
+    else:
+        want = negacyclic_mod(sums[0], sums[1], lit.t) if N <= 4096 else None
     return MKFCase(lit, o, k, nq - 1, keys, cts[0], cts[1], want)
 
 
@@ -161,7 +186,7 @@ def kklss_ckks_decode(case: KKLSSCase, out, lv, scale, ids=None):
     return kg.CKKSEncoder(lit.log_n).decode(kg.crt_centered(ph, lit.q[: lv + 1]), scale)
 
 
-def kklss_bfv_case(lit, k, seed=9) -> KKLSSCase:
+def kklss_bfv_case(lit, k, seed=9, sparse=False) -> KKLSSCase:
     o = Oracle.from_literal(lit)
     R = kg.RNS(o)
     N = o.n
@@ -173,14 +198,17 @@ def kklss_bfv_case(lit, k, seed=9) -> KKLSSCase:
         ct = np.zeros((k + 1, nq, N), np.uint64)
         tot = np.zeros(N, dtype=object)
         for i in range(k):
-            m = g.integers(0, lit.t, N)
+            m = sparse_message(g, N, lit.t) if sparse else g.integers(0, lit.t, N)
             tot = (tot + m) % lit.t
             c0, c1 = kg.kklss_encrypt(o, keys.public[i], bfv_plain(lit, m, nq), nq - 1, g)
             ct[0] = o.add(ct[0], c0)
             ct[i + 1] = c1
         cts.append(ct)
         sums.append(tot)
-    want = negacyclic_mod(sums[0], sums[1], lit.t) if N <= 4096 else None
+    if sparse:
+        want = sparse_negacyclic_mod(sums[0], sums[1], lit.t)
+    else:
+        want = negacyclic_mod(sums[0], sums[1], lit.t) if N <= 4096 else None
     return KKLSSCase(lit, o, k, nq - 1, keys, cts[0], cts[1], [1] * k, [1] * k, want)
 
 
