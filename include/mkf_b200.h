@@ -179,6 +179,22 @@ mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1
  * the ciphertext's is_ntt.  out: same components, lower level. */
 mkf_status mkf_rescale(mkf_ctx *ctx, const mkf_ct *in, double min_scale, mkf_ct *out,
                        void *stream);
+/* Rescale that allocates no device memory (no counterpart in the reference;
+ * it serves callers that cannot allocate on the call path, such as a server
+ * whose device-memory budget is fixed at start-up, or a host that must not
+ * pay the device-wide synchronization of cudaFree).  Divides each of npolys
+ * polynomials at `level` by its last modulus q_level (rounded), in the NTT
+ * domain when is_ntt, else the coefficient domain: d_in [npolys][level+1][N]
+ * and d_out [npolys][level][N] are caller-owned device buffers.  Temporaries
+ * live in one 8 MiB static device array shared by every call on a device:
+ * at most 2^20 / (2N) polynomials per call; larger requests return
+ * MKF_ERR_INVALID_ARG with a message.  The first call on a device looks up
+ * the array's device address, so make that call before any stream capture.
+ * Calls whose execution overlaps on the GPU (different streams, or several
+ * contexts on one device) race on the shared array and must be serialized by
+ * the caller.  Asynchronous on `stream`. */
+mkf_status mkf_rescale_noalloc(mkf_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, int npolys,
+                               int level, int is_ntt, void *stream);
 /* Host-buffer primitives (synchronous), for stage-level parity:
  *   basis 0 = Q, 1 = P, 2 = QMul; limbs [first, first+n_limbs).           */
 mkf_status mkf_ntt_host(mkf_ctx *ctx, int basis, int first, int n_limbs, const uint64_t *in,

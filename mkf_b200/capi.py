@@ -105,6 +105,7 @@ def lib():
         "mkf_ntt_host": (i, [vp, i, i, i, u64p, u64p, i]),
         "mkf_decompose_host": (i, [vp, i, i, u64p, u64p]),
         "mkf_switch_one_host": (i, [vp, i, i, u64p, u64p, i, u64p, u64p]),
+        "mkf_rescale_noalloc": (i, [vp, ctypes.c_void_p, ctypes.c_void_p, i, i, i, vp]),
         "mkf_profile_enable": (i, [vp, i]),
         "mkf_profile_kinds": (i, []),
         "mkf_profile_kind_name": (ctypes.c_char_p, [i]),

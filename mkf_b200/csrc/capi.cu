@@ -123,6 +123,19 @@ bool same_ids(const std::vector<int32_t> &a, const std::vector<int32_t> &b) { re
 
 } // namespace
 
+namespace mkf {
+// accessors for entry points defined in other translation units
+const Context &ctx_context(const mkf_ctx *ctx) { return ctx->c; }
+cudaStream_t ctx_stream(const mkf_ctx *ctx, void *stream) {
+    return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+void ctx_set_error(const mkf_ctx *ctx, const std::string &msg) {
+    mkf_ctx *m = const_cast<mkf_ctx *>(ctx);
+    std::lock_guard<std::mutex> g(m->err_mu);
+    m->err = msg;
+}
+} // namespace mkf
+
 extern "C" {
 
 const char *mkf_version(void) { return "mkf_b200 0.1 (sm_100a)"; }
