@@ -32,7 +32,7 @@ struct DevModulus {
     uint64_t last;    // psi^-1_rev[1] * N^-1 mod q (last inverse stage)
     uint64_t last_sh;
     double qd;        // (double)q, as the reference's float64 correction uses
-    uint64_t pad;
+    uint64_t one_sh;  // floor(2^64 / q): Shoup companion of 1
 };
 
 // A twiddle with its Shoup companion, loaded as one 16-byte word.
@@ -90,6 +90,15 @@ MKF_DEV uint64_t add_mod(uint64_t a, uint64_t b, uint64_t q) {
 }
 MKF_DEV uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t q) {
     return a >= b ? a - b : a + q - b;
+}
+// any 64-bit x -> [0,2q): Shoup product with 1 (one_sh = floor(2^64/q))
+MKF_DEV uint64_t reduce_2q(uint64_t x, uint64_t q, uint64_t one_sh) {
+    return x - __umul64hi(x, one_sh) * q;
+}
+// any 64-bit x -> [0,q)
+MKF_DEV uint64_t reduce_any(uint64_t x, uint64_t q, uint64_t one_sh) {
+    const uint64_t r = reduce_2q(x, q, one_sh);
+    return r >= q ? r - q : r;
 }
 // [0,4q) -> [0,q)
 MKF_DEV uint64_t reduce4(uint64_t x, uint64_t q) {

@@ -302,6 +302,7 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         d.ninv = h_invmod((uint64_t)N, qq);
         d.ninv_sh = h_shoup(d.ninv, qq);
         d.qd = (double)qq;
+        d.one_sh = h_shoup(1, qq);
         uint64_t g = h_primitive_root(qq);
         uint64_t psi = h_powmod(g, (qq - 1) / (2ull * N), qq);
         uint64_t ipsi = h_invmod(psi, qq);

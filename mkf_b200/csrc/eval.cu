@@ -132,7 +132,7 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     uint64_t *coeff = bfv ? nullptr : ar.take(2 * kk * poly);
     uint64_t *dig = ar.take(2 * kk * beta * qp);
     uint64_t *acc = ar.take(4 * kk * qp);
-    uint64_t *tmp = ar.take(4 * kk * poly);
+    uint64_t *tmp = ar.take(4 * poly);
     uint64_t *F = ar.take(4 * poly);
     uint64_t *mu = ar.take(3 * poly);
     uint64_t *rcoef = bfv ? nullptr : ar.take(poly);
@@ -154,7 +154,13 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         d2d2(coeff, poly, left.data + left.cs, left.cs, poly, k, st);
         d2d2(coeff + kk * poly, poly, right.data + right.cs, right.cs, poly, k, st);
         ntt_inverse(c, lsq(coeff, poly, L1), 2 * k, st);
-        decompose_ntt(c, coeff, poly, 0, level, 1, beta, dig, 2 * k, dscr, st);
+        OwnNtt own;
+        own.p[0] = left.data + left.cs;
+        own.p[1] = right.data + right.cs;
+        own.pstride[0] = left.cs;
+        own.pstride[1] = right.cs;
+        own.split = k;
+        decompose_ntt(c, coeff, poly, 0, level, 1, beta, dig, 2 * k, dscr, st, &own);
     } else {
         decompose_ntt(c, left.data + left.cs, left.cs, 0, level, 1, beta, dig, k, dscr, st);
         decompose_ntt(c, right.data + right.cs, right.cs, 0, level, 1, beta, dig + kk * beta * qp, k,
@@ -184,8 +190,18 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     ip.nP = nP;
     launch_ip(c, ip, st);
 
-    // 3. ModDown and fold: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1
-    moddown_prepare(c, st, acc, qp, 4 * k, L1, !bfv, tmp);
+    // 3. ModDown and fold: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1.
+    // Each party's P part is lifted exactly (ModUp per accumulator, as the
+    // reference's per-key ModDown does); the lifts are then summed mod q and
+    // transformed once per output, which equals the sum of the per-party
+    // ModDowns exactly because both NTT and P^-1 are linear mod q.
+    if (!bfv)
+        ntt_inverse(c, lsp_of_qp(c, acc, qp, L1), 4 * k, st);
+    else
+        ntt_inverse(c, lsqp(c, acc, qp, L1), 4 * k, st);
+    launch_modup_sum(c, c.p_to_q, acc + (long long)L1 * N, qp, 4 * qp, k, tmp, poly, 0, L1,
+                     qmap(L1), 4, st);
+    if (!bfv) ntt_forward(c, lsq(tmp, poly, L1), 4, st);
     d2d2(F, 2 * poly, left.data, left.cs, poly, 1, st);
     d2d2(F + 2 * poly, 2 * poly, right.data, right.cs, poly, 1, st);
     cudaMemsetAsync(F + poly, 0, poly * 8, st);
@@ -193,8 +209,8 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     {
         CombineSpec s = pdown(c, acc, qp, tmp, poly, F, poly, 1);
         s.x_tstride = 4 * qp;
-        s.y_tstride = 4 * poly;
         s.terms = k;
+        s.y_single = 1;
         launch_moddown_combine(c, s, L1, qmap(L1), 4, st);
     }
 
@@ -241,7 +257,14 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         }
     }
     // relinearization key switch of mu2 (coefficient domain input)
-    decompose_ntt(c, bfv ? mu2 : rcoef, poly, 0, level, 1, beta, rdig, 1, dscr, st);
+    {
+        OwnNtt own;
+        own.p[0] = mu2;
+        own.pstride[0] = poly;
+        own.split = 1;
+        decompose_ntt(c, bfv ? mu2 : rcoef, poly, 0, level, 1, beta, rdig, 1, dscr, st,
+                      bfv ? nullptr : &own);
+    }
     {
         IpArgs r;
         r.A = rdig;

@@ -138,7 +138,7 @@ size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int
 
 void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
                    int level, int gamma, int ndigits, uint64_t *out, int npolys,
-                   uint64_t *scratch, cudaStream_t st) {
+                   uint64_t *scratch, cudaStream_t st, const OwnNtt *own) {
     if (ndigits <= 0 || npolys <= 0) return;
     const int L1 = level + 1, limbs = L1 + c.nP;
     const long long qp = (long long)limbs * c.N;
@@ -168,6 +168,7 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     src.alpha = alpha;
     src.level = level;
     src.nQ = c.nQ;
+    if (own && !ring_r) src.own = *own;
     ntt_forward_digits(c, src, out, npolys, st);
 }
 
@@ -294,6 +295,76 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
         modup_kernel<64><<<grid, kBlock, 0, st>>>(a);
 }
 
+// Summed ModUp: a thread owns one coefficient of one output polynomial and a
+// chunk of kSumChunk target limbs, and walks the terms, reconstructing each
+// term's y_i and correction once per chunk.
+constexpr int kSumChunk = 8;
+
+struct ModUpSumArgs {
+    ModUpTab tab;
+    const uint64_t *src;
+    long long src_pstride, src_tstride;
+    uint64_t *out;
+    long long out_pstride;
+    const DevModulus *mods;
+    ModMap tgt;
+    int row0, nt, N, terms, nchunks;
+};
+
+template <int MAXNS>
+__global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= a.N) return;
+    const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * kSumChunk;
+    const int nj = min(kSumChunk, a.nt - j0);
+    uint64_t acc[kSumChunk];
+#pragma unroll
+    for (int jj = 0; jj < kSumChunk; ++jj) acc[jj] = 0;
+    for (int t = 0; t < a.terms; ++t) {
+        const uint64_t *src = a.src + (long long)t * a.src_tstride + (long long)p * a.src_pstride;
+        uint64_t xs[MAXNS], y[MAXNS];
+#pragma unroll
+        for (int i = 0; i < MAXNS; ++i)
+            if (i < a.tab.ns) xs[i] = src[(long long)i * a.N + x];
+        const uint64_t v = reconstruct<MAXNS>(xs, a.tab, a.mods, y);
+#pragma unroll
+        for (int jj = 0; jj < kSumChunk; ++jj) {
+            if (jj < nj) {
+                const DevModulus &m = a.mods[a.tgt(j0 + jj)];
+                acc[jj] = add_mod(acc[jj], canon(multsum<MAXNS>(y, a.tab, a.row0 + j0 + jj, v, m), m.q),
+                                  m.q);
+            }
+        }
+    }
+    uint64_t *out = a.out + (long long)p * a.out_pstride + (long long)j0 * a.N + x;
+#pragma unroll
+    for (int jj = 0; jj < kSumChunk; ++jj)
+        if (jj < nj) out[(long long)jj * a.N] = acc[jj];
+}
+
+void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src,
+                      long long src_pstride, long long src_tstride, int terms, uint64_t *out,
+                      long long out_pstride, int row0, int nt, ModMap tgt, int npolys,
+                      cudaStream_t st) {
+    if (npolys <= 0 || nt <= 0) return;
+    const int nchunks = (nt + kSumChunk - 1) / kSumChunk;
+    ModUpSumArgs a{tab, src, src_pstride, src_tstride, out, out_pstride, c.d_mods, tgt,
+                   row0, nt, c.N, terms, nchunks};
+    ProfScope ps(c, PK_MODUP, st, 8.0 * c.N * npolys * ((double)tab.ns * terms + nt));
+    const dim3 grid = grid_for(c.N, npolys * nchunks);
+    note_launch();
+    if (tab.ns <= 4)
+        modup_sum_kernel<4><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 8)
+        modup_sum_kernel<8><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 16)
+        modup_sum_kernel<16><<<grid, kBlock, 0, st>>>(a);
+    else if (tab.ns <= 32)
+        modup_sum_kernel<32><<<grid, kBlock, 0, st>>>(a);
+    else
+        modup_sum_kernel<64><<<grid, kBlock, 0, st>>>(a);
+}
+
 // ----------------------------------------------------------------------------
 // ModDown combine
 // ----------------------------------------------------------------------------
@@ -307,6 +378,11 @@ __global__ void __launch_bounds__(kBlock) moddown_combine_kernel(CombineSpec a, 
     const long long o = (long long)l * N + i;
     const long long xo = (long long)p * a.x_pstride + o, yo = (long long)p * a.y_pstride + o;
     uint64_t r = 0;
+    if (a.y_single) {
+        uint64_t xs = 0;
+        for (int t = 0; t < a.terms; ++t) xs = add_mod(xs, a.x[xo + (long long)t * a.x_tstride], m.q);
+        r = mred(a.y[yo] + 2 * m.q - xs, c, m.q, m.qinv);
+    } else
     for (int t = 0; t < a.terms; ++t) {
         const uint64_t xv = a.x ? a.x[xo + (long long)t * a.x_tstride] : 0;
         const uint64_t yv = a.y[yo + (long long)t * a.y_tstride];

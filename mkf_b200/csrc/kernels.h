@@ -2,6 +2,7 @@
 #pragma once
 
 #include "context.h"
+#include "ntt.h"
 
 namespace mkf {
 
@@ -29,11 +30,12 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
 // digit, digits contiguous.  For logN >= 13 the digits are never stored in
 // the coefficient domain: a pre-pass writes y_i and the float64 correction
 // and the NTT column pass reconstructs each limb on load.  scratch must hold
-// decompose_ntt_scratch_words() words.
+// decompose_ntt_scratch_words() words.  `own` (optional) gives the inputs in
+// the NTT domain: each digit's own limbs are copied from there.
 size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys);
 void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
                    int level, int gamma, int ndigits, uint64_t *out, int npolys,
-                   uint64_t *scratch, cudaStream_t st);
+                   uint64_t *scratch, cudaStream_t st, const OwnNtt *own = nullptr);
 
 // Inner products of digit polynomials with key polynomials (Montgomery: B in
 // MForm):
@@ -68,16 +70,25 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
                   uint64_t *out, long long out_pstride, int row0, int nt, ModMap tgt, int canonical,
                   int npolys, cudaStream_t st);
 
+// out[p] = sum over t < terms of ModUp(src + t*src_tstride + p*src_pstride),
+// canonical, for npolys outputs (same table and target layout as launch_modup).
+void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src,
+                      long long src_pstride, long long src_tstride, int terms, uint64_t *out,
+                      long long out_pstride, int row0, int nt, ModMap tgt, int npolys,
+                      cudaStream_t st);
+
 // ModDown combine (basis_extension.go:203-229): r = MRed(y + 2q - x, negc[l])
 // = (x - y) * C^-1 over nl limbs of npolys polynomials (x == nullptr: x = 0).
 // r is summed over `terms` (x, y at +t*x_tstride / +t*y_tstride) before
-// being stored; accumulate adds into out.
+// being stored; with y_single, y is one term already summed over t, and
+// r = (sum_t x_t - y) * C^-1.  accumulate adds into out.
 struct CombineSpec {
     const uint64_t *x = nullptr;
     long long x_pstride = 0, x_tstride = 0;
     const uint64_t *y = nullptr;
     long long y_pstride = 0, y_tstride = 0;
     int terms = 1;
+    int y_single = 0;
     const uint64_t *negc = nullptr;
     uint64_t *out = nullptr;
     long long out_pstride = 0;

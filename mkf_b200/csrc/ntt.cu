@@ -13,6 +13,10 @@
 // folds in N^-1.  All products are Shoup products on the integer pipes.
 #include "ntt.h"
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "modup.cuh"
 
 namespace mkf {
@@ -26,7 +30,16 @@ struct NttArgs {
     const Tw *tw1;
     const Tw *tw2;
     int logN, n1, n2;
+    // row pass of gadget digits [poly][digit][limb]: skip each digit's own
+    // limbs (already final, copied by the column pass); 0 = transform all
+    int own_alpha = 0, own_ndigits = 0, own_level = 0;
 };
+
+// Number of source limbs of digit d (decomposeAndSplit's p0idxed - p0idxst,
+// basis_extension.go:428-450).
+MKF_DEV int digit_ns(int level, int alpha, int d) {
+    return (level > alpha * (d + 1) - 1 ? alpha - 2 : (level % alpha) - 1) + 2;
+}
 
 __device__ __forceinline__ void ct_bfly(uint64_t &U, uint64_t &V, const Tw w, uint64_t q) {
     uint64_t u = U >= 2 * q ? U - 2 * q : U;
@@ -41,6 +54,30 @@ __device__ __forceinline__ void gs_bfly(uint64_t &U, uint64_t &V, const Tw w, ui
     uint64_t y = shoup_lazy(U + 2 * q - V, w.w, w.ws, q);
     U = x;
     V = y;
+}
+
+// Lazy butterflies for moduli below 2^55, whose 64-bit words leave room for
+// unreduced sums across a whole phase.  Forward (Cooley-Tukey): with inputs
+// below 2q the U operand grows by at most 2q per stage (the Shoup product is
+// below 2q for any 64-bit V), so 16 stages stay below 36q < 2^64.  Inverse
+// (Gentleman-Sande): the bound b of the operands at most doubles per stage,
+// and U + b - V (b a multiple of q above V) keeps the difference positive;
+// with inputs below 2q, 8 stages stay below 512q < 2^64, and each phase
+// starts again from [0,2q).  Larger moduli use the Harvey butterflies above.
+constexpr uint64_t kLazyBound = 1ull << 55;
+
+__device__ __forceinline__ void ct_bfly_lazy(uint64_t &U, uint64_t &V, const Tw w, uint64_t q) {
+    const uint64_t v = shoup_lazy(V, w.w, w.ws, q);
+    const uint64_t u = U;
+    U = u + v;
+    V = u + 2 * q - v;
+}
+
+__device__ __forceinline__ void gs_bfly_lazy(uint64_t &U, uint64_t &V, const Tw w, uint64_t q,
+                                             uint64_t bias) {
+    const uint64_t x = U + V;
+    V = shoup_lazy(U + bias - V, w.w, w.ws, q);
+    U = x;
 }
 
 // MODE 0: whole limb in one tile. MODE 1: column pass. MODE 2: row pass.
@@ -279,26 +316,36 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid) {
     }
 }
 
-template <int LOGS, bool COLS, bool REDUCE>
-MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, uint64_t q) {
+// Store reductions: none, [0,4q) -> [0,q), any -> [0,q), any -> [0,2q).
+enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q };
+
+template <int LOGS, bool COLS>
+MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const DevModulus &md,
+                        StoreRed red) {
     constexpr int S = 1 << LOGS, C = kTile / S;
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const int idx = e * kPhaseThreads + tid;
+        uint64_t v;
+        long long o;
         if (COLS) {
             const int r = idx / C, cc = idx % C;
-            uint64_t v = s[saddr<S>(cc, r)];
-            data[blockIdx.x * C + r * R + cc] = REDUCE ? reduce4(v, q) : v;
+            v = s[saddr<S>(cc, r)];
+            o = blockIdx.x * C + r * R + cc;
         } else {
             const int cc = idx / S, j = idx % S;
-            uint64_t v = s[saddr<S>(cc, j)];
-            data[(long long)blockIdx.x * kTile + idx] = REDUCE ? reduce4(v, q) : v;
+            v = s[saddr<S>(cc, j)];
+            o = (long long)blockIdx.x * kTile + idx;
         }
+        if (red == kRed4) v = reduce4(v, md.q);
+        else if (red == kRedAny) v = reduce_any(v, md.q, md.one_sh);
+        else if (red == kRed2q) v = reduce_2q(v, md.q, md.one_sh);
+        data[o] = v;
     }
 }
 
 // The butterfly passes of a forward phase on the tile in shared memory.
-template <int LOGS>
+template <int LOGS, bool LAZY>
 MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
     uint64_t v[8];
@@ -315,7 +362,10 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t) {
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
                     const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
-                    ct_bfly(v[r], v[r + stride], ldtw(tw + (1 << st) + i), q);
+                    if (LAZY)
+                        ct_bfly_lazy(v[r], v[r + stride], ldtw(tw + (1 << st) + i), q);
+                    else
+                        ct_bfly(v[r], v[r + stride], ldtw(tw + (1 << st) + i), q);
                 }
             }
         }
@@ -332,29 +382,65 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     const int limbs = a.ls.limbs;
     const int poly = blockIdx.y / limbs, l = blockIdx.y % limbs;
     const int m = a.ls.mod_of(l);
-    const uint64_t q = a.mods[m].q;
+    const DevModulus md = a.mods[m];
+    const uint64_t q = md.q;
+    const bool lazy = q < kLazyBound;
     const int N = 1 << a.logN;
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    if (!COLS && a.own_alpha) {
+        const int d = (blockIdx.y / limbs) % a.own_ndigits, start = d * a.own_alpha;
+        if (l < a.ls.nq && l >= start && l < start + digit_ns(a.own_level, a.own_alpha, d)) return;
+    }
     tile_load<LOGS, COLS>(s, data, R, tid);
     __syncthreads();
     const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
                         : a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-    fwd_passes<LOGS>(s, tw, q, c, t);
+    if (lazy)
+        fwd_passes<LOGS, true>(s, tw, q, c, t);
+    else
+        fwd_passes<LOGS, false>(s, tw, q, c, t);
     __syncthreads();
-    tile_store<LOGS, COLS, !COLS>(s, data, R, tid, q);
+    tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedNone : lazy ? kRedAny : kRed4);
 }
+
+MKF_DEV void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+MKF_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND> MKF_DEV void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+// (lo, hi) += a * b on 128 bits
+MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
+    asm("mad.lo.cc.u64 %0, %2, %3, %0;\n\tmadc.hi.u64 %1, %2, %3, %1;"
+        : "+l"(lo), "+l"(hi)
+        : "l"(a), "l"(b));
+}
+
+// Dynamic shared memory of the digit column pass: the NTT tile, two staging
+// tiles for y_i and one byte per word for the float64 correction.
+constexpr size_t kDigitsSmem = 3 * kTile * sizeof(uint64_t) + kTile;
 
 // Column pass of the NTT of gadget digits with the decomposition fused into
 // the load: every word of the tile is reconstructed from the digit's y_i and
 // float64 correction v (multSum, basis_extension.go:581-646), copied from an
 // own limb, or copied raw from a one-limb digit, instead of being read back
 // from a stored digit polynomial.  Grid rows enumerate (poly, digit, limb).
+// The y_i tiles are streamed into shared memory with asynchronous copies,
+// two in flight, so that the multiply-accumulate never waits on single loads.
+// multSum's 128-bit sum needs no reduction on the way: its high word stays
+// below ns * q_i * p_j / 2^64 < p_j.
 template <int LOGS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    __shared__ uint64_t s[kTile];
+    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t *s = dsm;
+    uint64_t *stg = dsm + kTile;
+    uint8_t *vb = reinterpret_cast<uint8_t *>(dsm + 3 * kTile);
     __shared__ uint64_t tq[8], tv[9];
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y / limbs, l = blockIdx.y % limbs;
@@ -365,71 +451,100 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     const int N = 1 << a.logN, R = 1 << a.n2;
     const int L1 = src.level + 1;
     const int start = d * src.alpha;
-    const int ns = (src.level > src.alpha * (d + 1) - 1 ? src.alpha - 2 : (src.level % src.alpha) - 1) + 2;
-    const int mode = ns == 1 ? 0 : (l < L1 && l >= start && l < start + ns) ? 1 : 2;
+    const int ns = digit_ns(src.level, src.alpha, d);
+    const bool own_limb = l < L1 && l >= start && l < start + ns;
+    const int mode = ns == 1 ? 0 : own_limb ? 1 : 2;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
-    if (mode == 2 && tid < 2 * ns + 1) {
-        const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
-        const int row = l < L1 ? l : src.nQ + (l - L1);
-        if (tid < ns)
-            tq[tid] = tb->qmod[row * ns + tid];
-        else
-            tv[tid - ns] = tb->vq[row * (ns + 1) + (tid - ns)];
-    }
-    __syncthreads();
-    const uint64_t *xp = src.x + (long long)poly * src.x_pstride;
-    const uint64_t *yp = src.y + (long long)pd * src.alpha * N;
-    const uint8_t *vp = src.v + (long long)pd * N;
-    const uint64_t *xs = xp + (long long)(mode == 0 ? start : l) * N;
+    if (own_limb && src.own.p[0]) {
+        // the digit's own limb is the input limb itself: copy its NTT form
+        const int gp = src.poly0 + poly;
+        const uint64_t *xn = (gp < src.own.split
+                                  ? src.own.p[0] + (long long)gp * src.own.pstride[0]
+                                  : src.own.p[1] + (long long)(gp - src.own.split) * src.own.pstride[1]) +
+                             (long long)l * N;
+        uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        const int idx = e * kPhaseThreads + tid;
-        const int r = idx / C, cc = idx % C;
-        const int coef = blockIdx.x * C + r * R + cc;
-        uint64_t val;
-        if (mode != 2) {
-            val = mred(xs[coef], md.mont1, q, md.qinv);
-        } else {
-            uint64_t lo = 0, hi = 0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (i < ns) {
-                    const uint64_t y = yp[(long long)i * N + coef], b = tq[i];
-                    const uint64_t pl = y * b, ph = __umul64hi(y, b);
-                    const uint64_t nl = lo + pl;
-                    hi += ph + (nl < lo ? 1 : 0);
-                    lo = nl;
-                }
-            }
-            const uint64_t h = __umul64hi(lo * md.qinv, q);
-            val = canon3(hi - h + q + tv[vp[coef]], q);
+        for (int e = 0; e < 8; ++e) {
+            const int idx = e * kPhaseThreads + tid;
+            const int coef = blockIdx.x * C + (idx / C) * R + idx % C;
+            dst[coef] = xn[coef];
         }
-        s[saddr<S>(cc, r)] = val;
+        return;
+    }
+    if (mode == 2) {
+        if (tid < 2 * ns + 1) {
+            const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
+            const int row = l < L1 ? l : src.nQ + (l - L1);
+            if (tid < ns)
+                tq[tid] = tb->qmod[row * ns + tid];
+            else
+                tv[tid - ns] = tb->vq[row * (ns + 1) + (tid - ns)];
+        }
+        const uint64_t *yp = src.y + (long long)pd * src.alpha * N + blockIdx.x * C;
+        const uint8_t *vp = src.v + (long long)pd * N + blockIdx.x * C;
+        // tile word w = r*C + cc sits at coefficient r*R + cc of the column tile
+        auto issue = [&](int i, uint64_t *buf) {
+            const uint64_t *g = yp + (long long)i * N;
+#pragma unroll
+            for (int k = 0; k < kTile / 2 / kPhaseThreads; ++k) {
+                const int w = 2 * (k * kPhaseThreads + tid);
+                cp_async16(buf + w, g + (w / C) * R + w % C);
+            }
+            cp_async_commit();
+        };
+        if (tid < kTile / 16) {
+            const int b = 16 * tid;
+            cp_async16(vb + b, vp + (b / C) * R + b % C);
+        }
+        issue(0, stg);
+        issue(1, stg + kTile);
+        uint64_t lo[8], hi[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) lo[e] = hi[e] = 0;
+        for (int i = 0; i < ns; ++i) {
+            if (i + 1 < ns)
+                cp_async_wait<1>();
+            else
+                cp_async_wait<0>();
+            __syncthreads();
+            const uint64_t *buf = stg + (i & 1) * kTile;
+            const uint64_t b = tq[i];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) mac128(lo[e], hi[e], buf[e * kPhaseThreads + tid], b);
+            __syncthreads();
+            if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int idx = e * kPhaseThreads + tid;
+            const uint64_t h = __umul64hi(lo[e] * md.qinv, q);
+            s[saddr<S>(idx % C, idx / C)] = canon3(hi[e] - h + q + tv[vb[idx]], q);
+        }
+    } else {
+        const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)(mode == 0 ? start : l) * N;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int idx = e * kPhaseThreads + tid;
+            const int r = idx / C, cc = idx % C;
+            s[saddr<S>(cc, r)] = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
+        }
     }
     __syncthreads();
-    fwd_passes<LOGS>(s, a.tw1 + (size_t)m * (1 << a.n1), q, c, t);
+    if (q < kLazyBound)
+        fwd_passes<LOGS, true>(s, a.tw1 + (size_t)m * (1 << a.n1), q, c, t);
+    else
+        fwd_passes<LOGS, false>(s, a.tw1 + (size_t)m * (1 << a.n1), q, c, t);
     __syncthreads();
     uint64_t *data = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N;
-    tile_store<LOGS, true, false>(s, data, R, tid, q);
+    tile_store<LOGS, true>(s, data, R, tid, md, kRedNone);
 }
 
-template <int LOGS, bool COLS>
-__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
-    constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S, NP = (LOGS + 2) / 3;
-    __shared__ uint64_t s[kTile];
-    const int limbs = a.ls.limbs;
-    const int poly = blockIdx.y / limbs, l = blockIdx.y % limbs;
-    const int m = a.ls.mod_of(l);
-    const DevModulus md = a.mods[m];
+// The butterfly passes of an inverse phase.  COLS: the second (last) inverse
+// phase, whose global stage 0 folds in N^-1 and leaves canonical values.
+template <int LOGS, bool COLS, bool LAZY>
+MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, int t) {
+    constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
     const uint64_t q = md.q;
-    const int N = 1 << a.logN;
-    const int R = 1 << a.n2;
-    uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
-    const int tid = threadIdx.x, c = tid / T, t = tid % T;
-    tile_load<LOGS, COLS>(s, data, R, tid);
-    __syncthreads();
-    const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
-                        : a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
     uint64_t v[8];
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
@@ -440,6 +555,8 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
             const int st = 3 * p + u;
             if (st < LOGS) {
                 const int stride = 1 << (LOGS - 1 - st - pass_pos<LOGS>(p));
+                // operands of this stage are below bias (lazy schedule)
+                const uint64_t bias = (2 * q) << (LOGS - 1 - st);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
@@ -447,12 +564,15 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
                     if (COLS && st == 0) {
                         // global stage 0: fold in N^-1
                         const uint64_t x = shoup(U + V, md.ninv, md.ninv_sh, q);
-                        const uint64_t y = shoup(U + 2 * q - V, md.last, md.last_sh, q);
+                        const uint64_t y = shoup(U + (LAZY ? bias : 2 * q) - V, md.last, md.last_sh, q);
                         U = x;
                         V = y;
                     } else {
                         const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
-                        gs_bfly(U, V, ldtw(tw + (1 << st) + i), q);
+                        if (LAZY)
+                            gs_bfly_lazy(U, V, ldtw(tw + (1 << st) + i), q, bias);
+                        else
+                            gs_bfly(U, V, ldtw(tw + (1 << st) + i), q);
                     }
                 }
             }
@@ -461,8 +581,32 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
         for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = v[r];
         __syncwarp();
     }
+}
+
+template <int LOGS, bool COLS>
+__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
+    constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
+    __shared__ uint64_t s[kTile];
+    const int limbs = a.ls.limbs;
+    const int poly = blockIdx.y / limbs, l = blockIdx.y % limbs;
+    const int m = a.ls.mod_of(l);
+    const DevModulus md = a.mods[m];
+    const bool lazy = md.q < kLazyBound;
+    const int N = 1 << a.logN;
+    const int R = 1 << a.n2;
+    uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
+    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    tile_load<LOGS, COLS>(s, data, R, tid);
     __syncthreads();
-    tile_store<LOGS, COLS, false>(s, data, R, tid, q);
+    const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
+                        : a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+    if (lazy)
+        inv_passes<LOGS, COLS, true>(s, tw, md, c, t);
+    else
+        inv_passes<LOGS, COLS, false>(s, tw, md, c, t);
+    __syncthreads();
+    // the first phase hands the second one values below 2q
+    tile_store<LOGS, COLS>(s, data, R, tid, md, (!COLS && lazy) ? kRed2q : kRedNone);
 }
 
 template <int LOG1, int LOG2>
@@ -528,6 +672,18 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
     }
 }
 
+// Opt a digit column kernel into kDigitsSmem bytes of dynamic shared memory,
+// once per kernel and device.
+template <typename K> static void digits_smem_attr(K kernel, int device) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), device);
+    if (done.count(key)) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDigitsSmem);
+    done.insert(key);
+}
+
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
                         cudaStream_t st) {
     const int L1 = src.level + 1, limbs = L1 + c.nP;
@@ -552,6 +708,12 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         sb.x = src.x + (long long)first_poly * src.x_pstride;
         sb.y = src.y + (long long)p0 * src.alpha * c.N;
         sb.v = src.v + (long long)p0 * c.N;
+        sb.poly0 = first_poly;
+        if (src.own.p[0]) {
+            b.own_alpha = src.alpha;
+            b.own_ndigits = src.ndigits;
+            b.own_level = src.level;
+        }
         const double bytes = 16.0 * c.N * limbs * npp;
         dim3 block(kPhaseThreads);
         note_launch(2);
@@ -561,7 +723,8 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_NTT_FWD_COL, st, bytes);                                            \
-            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(b, sb);                                 \
+            digits_smem_attr(ntt_fwd_digits_col<L1G>, c.device);                                   \
+            ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
         }                                                                                          \
         ProfScope ps(c, PK_NTT_FWD_ROW, st, bytes);                                                \
         ntt_fwd_phase<L2G, false><<<g2, block, 0, st>>>(b);                                        \
