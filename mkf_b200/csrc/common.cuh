@@ -79,6 +79,17 @@ MKF_DEV uint64_t shoup_lazy(uint64_t x, uint64_t w, uint64_t ws, uint64_t q) {
     uint64_t qh = __umul64hi(x, ws);
     return x * w - qh * q;
 }
+// floor(a*b / 2^64) - e with e in {0,1,2}: the three upper 32x32 partial
+// products only (the dropped low parts sum to less than 3 units).
+MKF_DEV uint64_t mulhi_approx(uint64_t a, uint64_t b) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+    const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    return (uint64_t)a1 * b1 + __umulhi(a1, b0) + __umulhi(a0, b1);
+}
+// x*w mod q in [0,4q) for any 64-bit x: Shoup with the approximate quotient.
+MKF_DEV uint64_t shoup_lazy4(uint64_t x, uint64_t w, uint64_t ws, uint64_t q) {
+    return x * w - mulhi_approx(x, ws) * q;
+}
 MKF_DEV uint64_t shoup(uint64_t x, uint64_t w, uint64_t ws, uint64_t q) {
     uint64_t r = shoup_lazy(x, w, ws, q);
     return r >= q ? r - q : r;

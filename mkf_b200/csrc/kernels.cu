@@ -298,7 +298,7 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
 // Summed ModUp: a thread owns one coefficient of one output polynomial and a
 // chunk of kSumChunk target limbs, and walks the terms, reconstructing each
 // term's y_i and correction once per chunk.
-constexpr int kSumChunk = 8;
+constexpr int kSumChunk = 12;
 
 struct ModUpSumArgs {
     ModUpTab tab;

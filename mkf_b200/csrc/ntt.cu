@@ -57,26 +57,28 @@ __device__ __forceinline__ void gs_bfly(uint64_t &U, uint64_t &V, const Tw w, ui
 }
 
 // Lazy butterflies for moduli below 2^55, whose 64-bit words leave room for
-// unreduced sums across a whole phase.  Forward (Cooley-Tukey): with inputs
-// below 2q the U operand grows by at most 2q per stage (the Shoup product is
-// below 2q for any 64-bit V), so 16 stages stay below 36q < 2^64.  Inverse
-// (Gentleman-Sande): the bound b of the operands at most doubles per stage,
-// and U + b - V (b a multiple of q above V) keeps the difference positive;
-// with inputs below 2q, 8 stages stay below 512q < 2^64, and each phase
-// starts again from [0,2q).  Larger moduli use the Harvey butterflies above.
+// unreduced sums across a whole phase.  Their Shoup products use the
+// three-partial-product quotient and land in [0,4q) for any 64-bit operand.
+// Forward (Cooley-Tukey): with inputs below 2q the U operand grows by at
+// most 4q per stage, so 16 stages stay below 66q < 2^64.  Inverse
+// (Gentleman-Sande): the bound b of the operands at most doubles per stage
+// (products stay below 4q <= b), and U + b - V (b a multiple of q above V)
+// keeps the difference positive; with inputs below 2q, 8 stages stay below
+// 512q < 2^64, and each phase starts again from [0,2q).  Larger moduli use
+// the Harvey butterflies above.
 constexpr uint64_t kLazyBound = 1ull << 55;
 
 __device__ __forceinline__ void ct_bfly_lazy(uint64_t &U, uint64_t &V, const Tw w, uint64_t q) {
-    const uint64_t v = shoup_lazy(V, w.w, w.ws, q);
+    const uint64_t v = shoup_lazy4(V, w.w, w.ws, q);
     const uint64_t u = U;
     U = u + v;
-    V = u + 2 * q - v;
+    V = u + 4 * q - v;
 }
 
 __device__ __forceinline__ void gs_bfly_lazy(uint64_t &U, uint64_t &V, const Tw w, uint64_t q,
                                              uint64_t bias) {
     const uint64_t x = U + V;
-    V = shoup_lazy(U + bias - V, w.w, w.ws, q);
+    V = shoup_lazy4(U + bias - V, w.w, w.ws, q);
     U = x;
 }
 
