@@ -59,6 +59,15 @@ def dist_env():
     return ws, rank, local
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, ncu, one launch)
+# of the fused decomposition + NTT column pass per source polynomial at
+# logN=16, L1=24, P=4 (C3 top level): one launch over 4 polynomials moved
+# 413.85 MB.  Integer-multiply pipe (sm__pipe_fmaheavy_cycles_active) and
+# issue utilisation from the same capture.
+DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 413.846528e6 / 4}
+DIGITS_COL_PIPES = {(16, 24, 4): {"fmaheavy_cycles_active_pct": 62.3, "issue_active_pct": 52.3}}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -353,11 +362,20 @@ def run_gpu(a):
     avg_ms = tk["ms"] / tk["launches"]
     bytes_per_launch = tk["bytes"] / tk["launches"]
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    shape = (lit.log_n, L1, nP)
+    traffic, pipes = None, None
+    if top[0] == "ntt_digits_col" and shape in DIGITS_COL_DRAM_PER_POLY:
+        # the fold launch (2k polynomials) and the relinearization launch (one)
+        # alternate, so a launch averages (2k+1)/2 source polynomials
+        traffic = DIGITS_COL_DRAM_PER_POLY[shape] * (2 * k + 1) / 2
+        pipes = DIGITS_COL_PIPES[shape]
     roofline = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
                 "share": tk["ms"] / sum(v["ms"] for v in kinds.values()),
+                "limiter": "integer multiply pipe (IMAD, fmaheavy), not HBM",
+                "int_pipes_ncu": pipes,
                 "timed_in": "plain region (one stream, no overlap)"}
 
     # ---- e2e through the C ABI with pinned host buffers -------------------------

@@ -28,7 +28,7 @@ struct ModUpTab {
 enum ProfKind : int {
     PK_NTT_FWD_COL, PK_NTT_FWD_ROW, PK_NTT_FWD_FULL, PK_NTT_INV_ROW, PK_NTT_INV_COL,
     PK_NTT_INV_FULL, PK_DECOMPOSE, PK_IP, PK_MODUP, PK_COMBINE, PK_TENSOR, PK_RESCALE,
-    PK_ELEMENTWISE, PK_COUNT
+    PK_ELEMENTWISE, PK_DIGITS_COL, PK_DIGITS_ROW, PK_COUNT
 };
 extern const char *const kProfNames[PK_COUNT];
 

@@ -716,7 +716,13 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
             b.own_ndigits = src.ndigits;
             b.own_level = src.level;
         }
-        const double bytes = 16.0 * c.N * limbs * npp;
+        // algorithmic bytes: the column pass writes every limb once and reads
+        // each (poly, digit)'s y_i and correction once (own limbs: read the
+        // NTT-domain input instead); the row pass reads and writes every limb
+        // it transforms.
+        const int own = src.own.p[0] ? std::min(src.alpha, L1) : 0;
+        const double bytes_col = (double)c.N * npp * (8.0 * limbs + 8.0 * src.alpha + 1.0);
+        const double bytes_row = 16.0 * c.N * npp * (limbs - own);
         dim3 block(kPhaseThreads);
         note_launch(2);
         switch (c.logN) {
@@ -724,11 +730,11 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
     case LN: {                                                                                     \
         dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
-            ProfScope ps(c, PK_NTT_FWD_COL, st, bytes);                                            \
+            ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
             digits_smem_attr(ntt_fwd_digits_col<L1G>, c.device);                                   \
             ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
         }                                                                                          \
-        ProfScope ps(c, PK_NTT_FWD_ROW, st, bytes);                                                \
+        ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         ntt_fwd_phase<L2G, false><<<g2, block, 0, st>>>(b);                                        \
         break;                                                                                     \
     }
