@@ -172,6 +172,47 @@ mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1
                               const mkf_kklss_keyset *ks, mkf_ct *out, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* batched form                                                         */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference, which runs one product per call
+ * serially; this is the batched mkf_mulrelin_batch form of the drop-in.
+ * A job is one MKF or KKLSS mult+relin, exactly as mkf_mkf_mulrelin /
+ * mkf_kklss_mulrelin would run it (same validation, bit-identical output).
+ * Jobs may mix party counts, levels, schemes and contexts (ring degrees) of
+ * one device. */
+#define MKF_JOB_MKF 1
+#define MKF_JOB_KKLSS 2
+typedef struct mkf_job {
+    int kind;                            /* MKF_JOB_MKF or MKF_JOB_KKLSS */
+    const mkf_ct *a, *b;                 /* operands */
+    const mkf_mkf_keyset *mkf_keys;      /* MKF_JOB_MKF */
+    const mkf_kklss_keyset *kklss_keys;  /* MKF_JOB_KKLSS */
+    int flags;                           /* MKF_JOB_MKF: MKF_FLAG_* */
+    mkf_ct *out;                         /* shaped as for the single call */
+    mkf_status status;                   /* written by mkf_batch_create */
+} mkf_job;
+typedef struct mkf_batch mkf_batch;
+#define MKF_BATCH_GRAPH 1 /* capture the whole batch into one CUDA graph */
+/* Validates every job (job.status; the first failure is returned and no
+ * plan is made), spreads the jobs over `lanes` concurrent streams of their
+ * context (longest job first onto the least-loaded lane), sizes each lane's
+ * scratch, and with MKF_BATCH_GRAPH captures the fork, all jobs and the join
+ * into one CUDA graph.  Output metadata (scale, party ids) is set here.
+ * Lanes and their scratch belong to the context and are shared by all plans
+ * of that context: launch such plans one after another on one stream. */
+mkf_status mkf_batch_create(mkf_ctx *ctx, mkf_job *jobs, int n, int lanes, int flags,
+                            mkf_batch **out);
+/* Runs the batch after the work already queued on `stream`; work queued on
+ * `stream` afterwards waits for every job.  A graph plan replays its graph
+ * (operand contents may change between launches; handles may not). */
+mkf_status mkf_batch_launch(mkf_batch *batch, void *stream);
+void mkf_batch_destroy(mkf_batch *batch);
+/* Kernels one launch of the plan issues. */
+uint64_t mkf_batch_kernels(const mkf_batch *batch);
+/* One-shot: create (no graph, min(n, 8) lanes), launch on `stream`, destroy. */
+mkf_status mkf_mulrelin_batch(mkf_ctx *ctx, mkf_job *jobs, int n, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* rescale and stage-level primitives                                   */
 /* ------------------------------------------------------------------ */
 /* Rescale by the last moduli while scale/q >= min_scale/2 (Lattigo

@@ -54,6 +54,19 @@ class ParamsDesc(ctypes.Structure):
     ]
 
 
+JOB_MKF, JOB_KKLSS = 1, 2
+BATCH_GRAPH = 1
+
+
+class Job(ctypes.Structure):
+    """struct mkf_job: one product of a batch."""
+    _fields_ = [
+        ("kind", ctypes.c_int), ("a", vp), ("b", vp),
+        ("mkf_keys", vp), ("kklss_keys", vp),
+        ("flags", ctypes.c_int), ("out", vp), ("status", ctypes.c_int),
+    ]
+
+
 _lib = None
 
 
@@ -106,6 +119,11 @@ def lib():
         "mkf_decompose_host": (i, [vp, i, i, u64p, u64p]),
         "mkf_switch_one_host": (i, [vp, i, i, u64p, u64p, i, u64p, u64p]),
         "mkf_rescale_noalloc": (i, [vp, ctypes.c_void_p, ctypes.c_void_p, i, i, i, vp]),
+        "mkf_batch_create": (i, [vp, ctypes.POINTER(Job), i, i, i, ctypes.POINTER(vp)]),
+        "mkf_batch_launch": (i, [vp, vp]),
+        "mkf_batch_destroy": (None, [vp]),
+        "mkf_batch_kernels": (ctypes.c_uint64, [vp]),
+        "mkf_mulrelin_batch": (i, [vp, ctypes.POINTER(Job), i, vp]),
         "mkf_profile_enable": (i, [vp, i]),
         "mkf_profile_kinds": (i, []),
         "mkf_profile_kind_name": (ctypes.c_char_p, [i]),

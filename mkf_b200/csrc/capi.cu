@@ -9,8 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/mkf_b200.h"
-#include "eval.h"
+#include "handles.h"
 
 namespace mkf {
 std::atomic<uint64_t> g_launches{0};
@@ -18,46 +17,7 @@ std::atomic<uint64_t> g_launches{0};
 
 using namespace mkf;
 
-struct mkf_ctx {
-    Context c;
-    cudaStream_t stream = nullptr;
-    std::mutex ws_mu;
-    std::map<cudaStream_t, std::unique_ptr<Workspace>> ws;
-    std::mutex err_mu;
-    std::string err;
-};
-
-struct mkf_key {
-    mkf_ctx *ctx = nullptr;
-    int kind = 0;
-    uint64_t *d = nullptr;
-    size_t words = 0;
-};
-
-struct mkf_ct {
-    mkf_ctx *ctx = nullptr;
-    int ncomp = 0, level = 0, is_ntt = 0;
-    double scale = 0;
-    std::vector<int32_t> ids;
-    uint64_t *d = nullptr;
-    size_t words() const { return (size_t)ncomp * (level + 1) * ctx->c.N; }
-    long long cs() const { return (long long)(level + 1) * ctx->c.N; }
-};
-
-struct mkf_mkf_keyset {
-    mkf_ctx *ctx = nullptr;
-    int k = 0;
-    std::vector<const uint64_t *> fold;
-    const uint64_t *relin = nullptr;
-};
-
-struct mkf_kklss_keyset {
-    mkf_ctx *ctx = nullptr;
-    const uint64_t *crs_u = nullptr;
-    std::map<int32_t, const mkf_key *> rlk;
-};
-
-namespace {
+namespace mkf {
 
 mkf_status fail(mkf_ctx *ctx, mkf_status s, const std::string &msg) {
     if (ctx) {
@@ -72,10 +32,6 @@ mkf_status cuda_check(mkf_ctx *ctx, const char *where) {
     if (e == cudaSuccess) return MKF_OK;
     return fail(ctx, e == cudaErrorMemoryAllocation ? MKF_ERR_OOM : MKF_ERR_CUDA,
                 std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-cudaStream_t pick(mkf_ctx *ctx, void *stream) {
-    return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
 }
 
 Workspace *workspace(mkf_ctx *ctx, cudaStream_t st) {
@@ -97,29 +53,218 @@ mkf_status status_of(const std::string &e) {
     return MKF_ERR_INVALID_ARG;
 }
 
-// Sizes the scratch with a dry run, grows the stream's workspace, then runs.
-template <class F> mkf_status run(mkf_ctx *ctx, cudaStream_t st, F &&f) {
-    cudaSetDevice(ctx->c.device);
-    Workspace *w = workspace(ctx, st);
+Call::~Call() {
+    if (!temps.empty()) {
+        cudaSetDevice(ctx->c.device);
+        cudaDeviceSynchronize();
+        for (mkf_ct *t : temps) mkf_ct_destroy(t);
+    }
+}
+
+mkf_status call_scratch(Call &call, size_t *words) {
     Arena dry;
     dry.dry = true;
-    std::string e = f(dry);
-    if (!e.empty()) return fail(ctx, status_of(e), e);
+    std::string e = call.body(dry, nullptr);
+    if (!e.empty()) return fail(call.ctx, status_of(e), e);
+    *words = dry.peak;
+    return MKF_OK;
+}
+
+mkf_status run_call(Call &call, cudaStream_t st) {
+    mkf_ctx *ctx = call.ctx;
+    cudaSetDevice(ctx->c.device);
+    Workspace *w = workspace(ctx, st);
+    size_t need = 0;
+    mkf_status s = call_scratch(call, &need);
+    if (s != MKF_OK) return s;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cap);
-    if (dry.peak > w->cap_words) {
+    if (need > w->cap_words) {
         if (cap != cudaStreamCaptureStatusNone)
             return fail(ctx, MKF_ERR_INVALID_ARG,
                         "workspace too small during stream capture; run the operation once first");
-        if (!w->reserve(dry.peak)) return fail(ctx, MKF_ERR_OOM, "workspace allocation failed");
+        if (!w->reserve(need)) return fail(ctx, MKF_ERR_OOM, "workspace allocation failed");
     }
     Arena a = w->arena();
-    e = f(a);
+    std::string e = call.body(a, st);
     if (!e.empty()) return fail(ctx, status_of(e), e);
-    return cuda_check(ctx, "kernel launch");
+    s = cuda_check(ctx, "kernel launch");
+    if (s == MKF_OK && call.commit) call.commit();
+    return s;
 }
 
-bool same_ids(const std::vector<int32_t> &a, const std::vector<int32_t> &b) { return a == b; }
+
+mkf_status prepare_mkf(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
+                       const mkf_mkf_keyset *ks, int flags, mkf_ct *out, Call &call) {
+    if (!ctx || !left || !right || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (ks->ctx != ctx || left->ctx != ctx || right->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const int k = ks->k;
+    if (left->ncomp != k + 1 || right->ncomp != k + 1)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
+    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
+    const int level = std::min(left->level, right->level);
+    int nb = 0;
+    double scale = left->scale * right->scale;
+    if (!bfv && (flags & MKF_FLAG_RESCALE)) {
+        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
+        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
+    }
+    const int lout = level - nb;
+    const int n_out = (flags & MKF_FLAG_MATERIALIZE) ? k + 1 : 2;
+    if (out->ncomp != n_out || out->level != lout)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(n_out) + " components at level " +
+                        std::to_string(lout));
+    if (!bfv && (!left->is_ntt || !right->is_ntt))
+        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF CKKS operands must be in the NTT domain");
+    if (bfv && (left->is_ntt || right->is_ntt))
+        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF BFV operands must be in the coefficient domain");
+    const Operand L{left->d, left->cs(), left->ncomp, left->level};
+    const Operand R{right->d, right->cs(), right->ncomp, right->level};
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) kp.p[i] = ks->fold[i];
+    const uint64_t *relin = ks->relin;
+    uint64_t *od = out->d;
+    const long long ocs = out->cs();
+    call.ctx = ctx;
+    call.body = [ctx, bfv, k, level, L, R, kp, relin, nb, n_out, od, ocs](Arena &a, cudaStream_t st) {
+        return mkf_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, L, R, kp, relin, nb, n_out,
+                            od, ocs);
+    };
+    std::vector<int32_t> ids = left->ids;
+    if (n_out == 2) ids.resize(1);
+    call.commit = [out, scale, bfv, ids]() {
+        out->scale = scale;
+        out->is_ntt = !bfv;
+        out->ids = ids;
+    };
+    const int beta = ctx->c.beta_of(level, 1);
+    call.cost = (2.0 * k + 1) * beta * (level + 1 + ctx->c.nP) * ctx->c.N;
+    return MKF_OK;
+}
+
+mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
+                         const mkf_kklss_keyset *ks, mkf_ct *out, Call &call) {
+    if (!ctx || !op0 || !op1 || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (ks->ctx != ctx || op0->ctx != ctx || op1->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
+    if (op0->is_ntt || op1->is_ntt)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "KKLSS operands must be in the coefficient domain");
+    std::vector<int32_t> u = op0->ids;
+    for (int32_t id : op1->ids)
+        if (std::find(u.begin(), u.end(), id) == u.end()) u.push_back(id);
+    const int k = (int)u.size();
+    if (k < 1 || k > kMaxParties) return fail(ctx, MKF_ERR_INVALID_ARG, "party count out of range");
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) {
+        auto it = ks->rlk.find(u[i]);
+        if (it == ks->rlk.end())
+            return fail(ctx, MKF_ERR_MISSING_KEY,
+                        "there is no relinearization key with id " + std::to_string(u[i]));
+        kp.p[i] = it->second->d;
+    }
+    const int level = std::min(op0->level, op1->level);
+    int nb = 0;
+    double scale = op0->scale * op1->scale;
+    if (!bfv) {
+        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
+        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
+    }
+    const int lout = level - nb;
+    if (out->ncomp != k + 1 || out->level != lout)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(k + 1) + " components at level " +
+                        std::to_string(lout));
+    call.ctx = ctx;
+    // operands whose party list differs from the union are copied into
+    // union-ordered temporaries (absent components are zero) on every issue
+    struct Align {
+        const uint64_t *src = nullptr;
+        long long src_cs = 0;
+        uint64_t *dst = nullptr;
+        std::vector<int> pos; // union position of each source party component
+    };
+    std::vector<Align> aligns;
+    Operand O[2];
+    const long long w = (long long)(level + 1) * ctx->c.N;
+    const mkf_ct *ops[2] = {op0, op1};
+    for (int j = 0; j < 2; ++j) {
+        const mkf_ct *op = ops[j];
+        if (op->ids == u) {
+            O[j] = Operand{op->d, op->cs(), op->ncomp, op->level};
+            continue;
+        }
+        mkf_ct *t = nullptr;
+        mkf_status s = mkf_ct_create(ctx, k + 1, level, 0, &t);
+        if (s != MKF_OK) return s;
+        call.temps.push_back(t);
+        Align al;
+        al.src = op->d;
+        al.src_cs = op->cs();
+        al.dst = t->d;
+        for (int32_t id : op->ids) al.pos.push_back((int)(std::find(u.begin(), u.end(), id) - u.begin()));
+        aligns.push_back(al);
+        O[j] = Operand{t->d, w, k + 1, level};
+    }
+    const int N = ctx->c.N;
+    (void)N;
+    const uint64_t *crs = ks->crs_u;
+    uint64_t *od = out->d;
+    const long long ocs = out->cs();
+    const Operand O0 = O[0], O1 = O[1];
+    call.body = [ctx, bfv, k, level, O0, O1, kp, crs, nb, od, ocs, aligns, w](Arena &a, cudaStream_t st) {
+        if (!a.dry) {
+            for (const Align &al : aligns) {
+                cudaMemsetAsync(al.dst, 0, (size_t)(k + 1) * w * 8, st);
+                cudaMemcpyAsync(al.dst, al.src, w * 8, cudaMemcpyDeviceToDevice, st);
+                for (size_t i = 0; i < al.pos.size(); ++i)
+                    cudaMemcpyAsync(al.dst + (long long)(al.pos[i] + 1) * w,
+                                    al.src + (long long)(i + 1) * al.src_cs, w * 8,
+                                    cudaMemcpyDeviceToDevice, st);
+            }
+        }
+        return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, O0, O1, kp, crs, nb, od, ocs);
+    };
+    call.commit = [out, u, scale]() {
+        out->ids = u;
+        out->scale = scale;
+        out->is_ntt = 0;
+    };
+    const int beta = ctx->c.beta_of(level, 2);
+    call.cost = 7.0 * k * beta * (level + 1 + ctx->c.nP) * ctx->c.N;
+    return MKF_OK;
+}
+
+cudaStream_t ctx_lane(mkf_ctx *ctx, int i) {
+    std::lock_guard<std::mutex> g(ctx->lanes_mu);
+    cudaSetDevice(ctx->c.device);
+    while ((int)ctx->lanes.size() <= i) {
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        ctx->lanes.push_back(s);
+    }
+    return ctx->lanes[i];
+}
+
+} // namespace mkf
+
+namespace {
+
+cudaStream_t pick(mkf_ctx *ctx, void *stream) {
+    return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+// Sizes the scratch with a dry run, grows the stream's workspace, then runs.
+template <class F> mkf_status run(mkf_ctx *ctx, cudaStream_t st, F &&f) {
+    Call call;
+    call.ctx = ctx;
+    call.body = [&](Arena &a, cudaStream_t) { return f(a); };
+    return run_call(call, st);
+}
 
 } // namespace
 
@@ -199,6 +344,7 @@ void mkf_ctx_destroy(mkf_ctx *ctx) {
     cudaSetDevice(ctx->c.device);
     cudaDeviceSynchronize();
     ctx->ws.clear();
+    for (cudaStream_t l : ctx->lanes) cudaStreamDestroy(l);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -380,47 +526,10 @@ void mkf_mkf_keyset_destroy(mkf_mkf_keyset *ks) { delete ks; }
 
 mkf_status mkf_mkf_mulrelin(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
                             const mkf_mkf_keyset *ks, int flags, mkf_ct *out, void *stream) {
-    if (!ctx || !left || !right || !ks || !out) return MKF_ERR_INVALID_ARG;
-    if (ks->ctx != ctx || left->ctx != ctx || right->ctx != ctx || out->ctx != ctx)
-        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
-    const int k = ks->k;
-    if (left->ncomp != k + 1 || right->ncomp != k + 1)
-        return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
-    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
-    const int level = std::min(left->level, right->level);
-    int nb = 0;
-    double scale = left->scale * right->scale;
-    if (!bfv && (flags & MKF_FLAG_RESCALE)) {
-        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
-        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
-    }
-    const int lout = level - nb;
-    const int n_out = (flags & MKF_FLAG_MATERIALIZE) ? k + 1 : 2;
-    if (out->ncomp != n_out || out->level != lout)
-        return fail(ctx, MKF_ERR_INVALID_ARG,
-                    "output must have " + std::to_string(n_out) + " components at level " +
-                        std::to_string(lout));
-    if (!bfv && (!left->is_ntt || !right->is_ntt))
-        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF CKKS operands must be in the NTT domain");
-    if (bfv && (left->is_ntt || right->is_ntt))
-        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF BFV operands must be in the coefficient domain");
-    Operand L{left->d, left->cs(), left->ncomp, left->level};
-    Operand R{right->d, right->cs(), right->ncomp, right->level};
-    KeyPtrs kp;
-    kp.k = k;
-    for (int i = 0; i < k; ++i) kp.p[i] = ks->fold[i];
-    cudaStream_t st = pick(ctx, stream);
-    mkf_status s = run(ctx, st, [&](Arena &a) {
-        return mkf_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, L, R, kp, ks->relin, nb,
-                            n_out, out->d, out->cs());
-    });
-    if (s == MKF_OK) {
-        out->scale = scale;
-        out->is_ntt = !bfv;
-        out->ids = left->ids;
-        if (n_out == 2) out->ids.resize(1);
-    }
-    return s;
+    Call call;
+    mkf_status s = prepare_mkf(ctx, left, right, ks, flags, out, call);
+    if (s != MKF_OK) return s;
+    return run_call(call, pick(ctx, stream));
 }
 
 mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out) {
@@ -458,79 +567,10 @@ mkf_status mkf_kklss_union(const mkf_ct *op0, const mkf_ct *op1, int32_t *ids, i
 
 mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
                               const mkf_kklss_keyset *ks, mkf_ct *out, void *stream) {
-    if (!ctx || !op0 || !op1 || !ks || !out) return MKF_ERR_INVALID_ARG;
-    if (ks->ctx != ctx || op0->ctx != ctx || op1->ctx != ctx || out->ctx != ctx)
-        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
-    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
-    if (op0->is_ntt || op1->is_ntt)
-        return fail(ctx, MKF_ERR_INVALID_ARG, "KKLSS operands must be in the coefficient domain");
-    std::vector<int32_t> u = op0->ids;
-    for (int32_t id : op1->ids)
-        if (std::find(u.begin(), u.end(), id) == u.end()) u.push_back(id);
-    const int k = (int)u.size();
-    if (k < 1 || k > kMaxParties) return fail(ctx, MKF_ERR_INVALID_ARG, "party count out of range");
-    KeyPtrs kp;
-    kp.k = k;
-    for (int i = 0; i < k; ++i) {
-        auto it = ks->rlk.find(u[i]);
-        if (it == ks->rlk.end())
-            return fail(ctx, MKF_ERR_MISSING_KEY,
-                        "there is no relinearization key with id " + std::to_string(u[i]));
-        kp.p[i] = it->second->d;
-    }
-    const int level = std::min(op0->level, op1->level);
-    int nb = 0;
-    double scale = op0->scale * op1->scale;
-    if (!bfv) {
-        if (level == 0) return fail(ctx, MKF_ERR_LEVEL, "cannot rescale: input already at level 0");
-        nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
-    }
-    const int lout = level - nb;
-    if (out->ncomp != k + 1 || out->level != lout)
-        return fail(ctx, MKF_ERR_INVALID_ARG,
-                    "output must have " + std::to_string(k + 1) + " components at level " +
-                        std::to_string(lout));
-    cudaStream_t st = pick(ctx, stream);
-    cudaSetDevice(ctx->c.device);
-    // align the operands to the union party list (absent components are zero)
-    std::vector<mkf_ct *> tmp;
-    auto align = [&](const mkf_ct *op, Operand &o) -> mkf_status {
-        if (op->ids == u) {
-            o = Operand{op->d, op->cs(), op->ncomp, op->level};
-            return MKF_OK;
-        }
-        mkf_ct *t = nullptr;
-        mkf_status s = mkf_ct_create(ctx, k + 1, level, 0, &t);
-        if (s != MKF_OK) return s;
-        tmp.push_back(t);
-        const long long w = (long long)(level + 1) * ctx->c.N;
-        cudaMemsetAsync(t->d, 0, t->words() * 8, st);
-        cudaMemcpy2DAsync(t->d, w * 8, op->d, op->cs() * 8, w * 8, 1, cudaMemcpyDeviceToDevice, st);
-        for (size_t i = 0; i < op->ids.size(); ++i) {
-            int pos = (int)(std::find(u.begin(), u.end(), op->ids[i]) - u.begin());
-            cudaMemcpyAsync(t->d + (long long)(pos + 1) * w, op->d + (long long)(i + 1) * op->cs(),
-                            w * 8, cudaMemcpyDeviceToDevice, st);
-        }
-        o = Operand{t->d, w, k + 1, level};
-        return MKF_OK;
-    };
-    Operand O0, O1;
-    mkf_status s = align(op0, O0);
-    if (s == MKF_OK) s = align(op1, O1);
-    if (s == MKF_OK) {
-        s = run(ctx, st, [&](Arena &a) {
-            return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, O0, O1, kp, ks->crs_u,
-                                  nb, out->d, out->cs());
-        });
-    }
-    if (!tmp.empty()) cudaStreamSynchronize(st);
-    for (mkf_ct *t : tmp) mkf_ct_destroy(t);
-    if (s == MKF_OK) {
-        out->ids = u;
-        out->scale = scale;
-        out->is_ntt = 0;
-    }
-    return s;
+    Call call;
+    mkf_status s = prepare_kklss(ctx, op0, op1, ks, out, call);
+    if (s != MKF_OK) return s;
+    return run_call(call, pick(ctx, stream));
 }
 
 mkf_status mkf_rescale(mkf_ctx *ctx, const mkf_ct *in, double min_scale, mkf_ct *out,

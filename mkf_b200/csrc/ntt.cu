@@ -686,6 +686,12 @@ template <typename K> static void digits_smem_attr(K kernel, int device) {
     done.insert(key);
 }
 
+void ntt_prepare(const Context &c) {
+    digits_smem_attr(ntt_fwd_digits_col<6>, c.device);
+    digits_smem_attr(ntt_fwd_digits_col<7>, c.device);
+    digits_smem_attr(ntt_fwd_digits_col<8>, c.device);
+}
+
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
                         cudaStream_t st) {
     const int L1 = src.level + 1, limbs = L1 + c.nP;

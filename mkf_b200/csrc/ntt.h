@@ -37,5 +37,8 @@ struct DigitSrc {
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
                         cudaStream_t st);
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
+// Sets the kernels' launch attributes for c's device (idempotent); called
+// before a stream capture so that nothing but launches happens inside it.
+void ntt_prepare(const Context &c);
 
 } // namespace mkf

@@ -291,6 +291,58 @@ class MKFEvaluator:
             self.params.handle, left.handle, right.handle, self.keys.handle, flags, out.handle, stream))
 
 
+class Batch:
+    """A batch plan (mkf_batch_create): many products over concurrent lanes,
+    optionally captured into one CUDA graph.  Jobs are
+    ("mkf", MKFEvaluator, left, right, out, rescale, materialize) or
+    ("kklss", RelinearizationKeySet, op0, op1, out); outputs are shaped as for
+    the single calls (see MKFEvaluator.output_level / Evaluator.MulRelinNew)."""
+
+    def __init__(self, params: Parameters, jobs, lanes: int = 8, graph: bool = True):
+        self.params = params
+        self._keep = list(jobs)  # handles must outlive the plan
+        arr = (capi.Job * max(1, len(jobs)))()
+        for i, j in enumerate(jobs):
+            if j[0] == "mkf":
+                _, ev, left, right, out, rescale, materialize = j
+                arr[i].kind = capi.JOB_MKF
+                arr[i].mkf_keys = ev.keys.handle
+                arr[i].flags = (capi.FLAG_RESCALE if rescale else 0) | \
+                    (capi.FLAG_MATERIALIZE if materialize else 0)
+            else:
+                _, rlk, left, right, out = j
+                arr[i].kind = capi.JOB_KKLSS
+                arr[i].kklss_keys = rlk.handle
+            arr[i].a, arr[i].b, arr[i].out = left.handle, right.handle, out.handle
+        self.jobs = arr
+        h = ctypes.c_void_p()
+        st = capi.lib().mkf_batch_create(params.handle, arr, len(jobs), lanes,
+                                        capi.BATCH_GRAPH if graph else 0, ctypes.byref(h))
+        capi.check(params.handle, st)
+        self.handle = h
+
+    def statuses(self):
+        return [int(self.jobs[i].status) for i in range(len(self._keep))]
+
+    def launch(self, stream=None):
+        capi.check(self.params.handle, capi.lib().mkf_batch_launch(self.handle, stream))
+
+    @property
+    def kernels(self) -> int:
+        return int(capi.lib().mkf_batch_kernels(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            capi.lib().mkf_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # stage-level primitives ------------------------------------------------------
 
 def ntt(params: Parameters, arr: np.ndarray, basis: str = "Q", first: int = 0, inverse=False):

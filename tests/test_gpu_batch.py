@@ -1,0 +1,130 @@
+"""Batch plans (mkf_batch_create / mkf_batch_launch, mkf_mulrelin_batch):
+every job of a mixed batch (party counts, levels, MKF and KKLSS, two ring
+degrees) must equal the single-call result bit for bit, eagerly and when
+replayed from the captured CUDA graph, including after the operands change."""
+import numpy as np
+import pytest
+
+from mkf_b200 import capi, params
+from mkf_b200 import evaluator as ev
+from tests.test_gpu_parity import gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _limbs(g, moduli, n, lead=()):
+    out = np.empty(tuple(lead) + (len(moduli), n), np.uint64)
+    for i, q in enumerate(moduli):
+        out[..., i, :] = g.integers(0, q, size=tuple(lead) + (n,), dtype=np.uint64)
+    return out
+
+
+class _Ring:
+    """Random keys for one ring: MKF key bundles per k and a KKLSS key set."""
+
+    def __init__(self, lit, seed, ks):
+        self.lit, self.P = lit, gpu(lit, "ckks")
+        self.g = np.random.default_rng(seed)
+        nQ, nP, N = len(lit.q), len(lit.p), lit.n
+        qp = list(lit.q) + list(lit.p)
+        beta1 = (nQ - 1 + nP) // nP
+
+        def swk():
+            return np.ascontiguousarray(_limbs(self.g, qp, N, (beta1, 2)))
+        self.mkf = {k: ev.MKFEvaluator(self.P, ev.MKFKeySet(self.P, [swk() for _ in range(k)], swk()))
+                    for k in ks}
+        beta2 = (nQ - 1 + nP // 2) // (nP // 2)
+        self.rlk = ev.RelinearizationKeySet(self.P, _limbs(self.g, qp, N, (beta2,)))
+        for pid in range(6):
+            self.rlk.AddRelinearizationKey(pid, np.ascontiguousarray(_limbs(self.g, qp, N, (3, beta2))))
+        self.E = ev.Evaluator(self.P)
+
+    def ct(self, ncomp, level, ntt, ids=None):
+        a = _limbs(self.g, self.lit.q[: level + 1], self.lit.n, (ncomp,))
+        return ev.Ciphertext.from_array(self.P, a, ntt, ids=ids, scale=self.lit.scale)
+
+
+def _make_jobs(r14, r13):
+    jobs, singles = [], []
+    for ring, k, level in [(r14, 2, 7), (r14, 3, 4), (r14, 1, 2), (r13, 2, 5), (r13, 3, 3), (r14, 2, 1)]:
+        E = ring.mkf[k]
+        left, right = ring.ct(k + 1, level, True), ring.ct(k + 1, level, True)
+        materialize = level % 2 == 1
+        lvl = E.output_level(left, right, True)
+        out = ev.Ciphertext(ring.P, k + 1 if materialize else 2, lvl, True)
+        jobs.append(("mkf", E, left, right, out, True, materialize))
+        singles.append(lambda E=E, l=left, r=right, m=materialize: E.MulRelinNew(l, r, True, m).download())
+    # KKLSS: one aligned pair and one pair needing the union alignment
+    for ring, ids0, ids1, level in [(r13, [0, 1], [0, 1], 4), (r14, [0, 2], [1, 2, 3], 5)]:
+        op0 = ring.ct(len(ids0) + 1, level, False, ids0)
+        op1 = ring.ct(len(ids1) + 1, level, False, ids1)
+        ref = ring.E.MulRelinNew(op0, op1, ring.rlk)
+        out = ev.Ciphertext(ring.P, ref.n_comp, ref.Level(), False)
+        jobs.append(("kklss", ring.rlk, op0, op1, out))
+        singles.append(lambda ring=ring, a=op0, b=op1: ring.E.MulRelinNew(a, b, ring.rlk).download())
+    return jobs, singles
+
+
+@pytest.fixture(scope="module")
+def rings():
+    r14 = _Ring(params.small("ckks", log_n=14, n_q=8, n_p=2, q_bits=45, first_bits=55, p_bits=55,
+                             scale_bits=45), 11, (1, 2, 3))
+    r13 = _Ring(params.small("ckks", log_n=13, n_q=6, n_p=2, q_bits=45, first_bits=55, p_bits=55,
+                             scale_bits=45), 12, (2, 3))
+    return r14, r13
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_matches_single_calls(rings, graph):
+    jobs, singles = _make_jobs(*rings)
+    want = [f() for f in singles]
+    b = ev.Batch(rings[0].P, jobs, lanes=3, graph=graph)
+    assert b.statuses() == [0] * len(jobs)
+    for rep in range(2):
+        b.launch()
+        ev.capi.lib()  # keep the binding loaded
+        import torch
+        torch.cuda.synchronize()
+        for i, j in enumerate(jobs):
+            got = j[4].download()
+            assert np.array_equal(got, want[i]), f"job {i} differs (graph={graph}, launch {rep})"
+    assert b.kernels > 0
+    # new operand contents, same handles: the plan recomputes
+    g = np.random.default_rng(99)
+    for j in jobs:
+        for op in (j[2], j[3]):
+            lit = rings[0].lit if op.params is rings[0].P else rings[1].lit
+            op.upload(_limbs(g, lit.q[: op.Level() + 1], lit.n, (op.n_comp,)))
+    want2 = [f() for f in singles]
+    b.launch()
+    import torch
+    torch.cuda.synchronize()
+    for i, j in enumerate(jobs):
+        assert np.array_equal(j[4].download(), want2[i]), f"job {i} differs after new operands"
+    b.close()
+
+
+def test_batch_rejects_invalid_job(rings):
+    r14 = rings[0]
+    E = r14.mkf[2]
+    left, right = r14.ct(3, 5, True), r14.ct(3, 5, True)
+    bad_out = ev.Ciphertext(r14.P, 2, 5, True)  # wrong level: rescale lowers it
+    with pytest.raises(capi.MKFError, match="output must have"):
+        ev.Batch(r14.P, [("mkf", E, left, right, bad_out, True, False)], lanes=2, graph=True)
+
+
+def test_one_shot_batch(rings):
+    jobs, singles = _make_jobs(*rings)
+    want = [f() for f in singles]
+    arr = (capi.Job * len(jobs))()
+    for i, j in enumerate(jobs):
+        if j[0] == "mkf":
+            arr[i].kind, arr[i].mkf_keys = capi.JOB_MKF, j[1].keys.handle
+            arr[i].flags = capi.FLAG_RESCALE | (capi.FLAG_MATERIALIZE if j[6] else 0)
+        else:
+            arr[i].kind, arr[i].kklss_keys = capi.JOB_KKLSS, j[1].handle
+        arr[i].a, arr[i].b, arr[i].out = j[2].handle, j[3].handle, j[4].handle
+    P = rings[0].P
+    capi.check(P.handle, capi.lib().mkf_mulrelin_batch(P.handle, arr, len(jobs), None))
+    for i, j in enumerate(jobs):
+        assert np.array_equal(j[4].download(), want[i]), f"job {i} differs"
