@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--level", type=int, default=-1)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--mix", type=int, default=512,
+                    help="products in the mixed batch (k in {2,4,8,16}, logN in {14,15}, "
+                         "level uniform over [1,L]); 0 skips it")
+    ap.add_argument("--lanes", default="4,8,16", help="lane counts the batch autotuner tries")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -426,6 +430,8 @@ def run_gpu(a):
                "h2d_bytes_per_step": 2 * a.batch * words_in * 8,
                "d2h_bytes_per_step": a.batch * words_out * 8}
 
+    mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a.config, k, level)
@@ -449,6 +455,7 @@ def run_gpu(a):
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roofline,
+            "batched_mix": mix,
             "kernels": kinds,
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -460,6 +467,100 @@ def run_gpu(a):
 
 
 import ctypes  # noqa: E402
+
+
+def run_mix(a, local, rank, barrier, max_over_ranks):
+    """The mixed batch: `a.mix` MK-CKKS products (MKF construction, rescale and
+    materialize), k uniform over {2,4,8,16}, ring uniform over the logN=14
+    and logN=15 sets, level uniform over [1,L].  Plain = one product per call
+    on one stream; batched = the plan replayed from its CUDA graph, lanes
+    picked by timing each candidate.  Synthetic uniform words (values below
+    every modulus of the ring), keys shared per (ring, k)."""
+    import torch
+    from mkf_b200 import capi, params
+    from mkf_b200 import evaluator as ev
+    g = np.random.Generator(np.random.PCG64(777 + rank))
+    rings = {}
+    for name in ("S14", "S15"):
+        lit = params.get("ckks", name)
+        P = ev.Parameters(lit, "ckks", device=local)
+        nQ, nP, N = len(lit.q), len(lit.p), lit.n
+        qmin = min(min(lit.q), min(lit.p))
+        beta = (nQ + nP - 1) // nP
+        key = g.integers(0, qmin, size=(beta, 2, nQ + nP, N), dtype=np.uint64)
+        evs = {k: ev.MKFEvaluator(P, ev.MKFKeySet(P, [key] * k, key)) for k in (2, 4, 8, 16)}
+        ctbuf = g.integers(0, qmin, size=17 * nQ * N, dtype=np.uint64)
+        rings[name] = (lit, P, evs, ctbuf)
+    items, shapes = [], []
+    for _ in range(a.mix):
+        name = ("S14", "S15")[int(g.integers(2))]
+        lit, P, evs, ctbuf = rings[name]
+        k = int(g.choice([2, 4, 8, 16]))
+        level = int(g.integers(1, lit.max_level + 1))
+        words = (k + 1) * (level + 1) * lit.n
+        ops = []
+        for _ in range(2):
+            c = ev.Ciphertext(P, k + 1, level, True, scale=lit.scale)
+            c.upload(ctbuf[:words].reshape(k + 1, level + 1, lit.n))
+            ops.append(c)
+        E = evs[k]
+        out = ev.Ciphertext(P, k + 1, E.output_level(ops[0], ops[1], True), True)
+        items.append(("mkf", E, ops[0], ops[1], out, True, True))
+        shapes.append((name, k, level))
+    P0 = rings["S14"][1]
+    s0 = torch.cuda.Stream()
+    cs = ctypes_stream(s0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    L = capi.lib()
+
+    def plain_pass():
+        for it in items:
+            it[1].MulRelin(it[2], it[3], it[4], rescale=True, materialize=True, stream=cs)
+
+    def timed(fn, reps):
+        for _ in range(max(1, a.warmup)):
+            fn()
+        barrier()
+        e0.record(s0)
+        for _ in range(reps):
+            fn()
+        e1.record(s0)
+        e1.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)) / reps
+
+    reps = max(2, a.steps // 2)
+    plain_ms = timed(plain_pass, reps)
+    # autotune the lane count: time each candidate plan, keep the fastest
+    tried = {}
+    best = None
+    for lanes in [int(x) for x in a.lanes.split(",") if x]:
+        b = ev.Batch(P0, items, lanes=lanes, graph=True)
+        ms = timed(lambda: b.launch(cs), reps)
+        tried[lanes] = ms
+        if best is None or ms < best[1]:
+            if best is not None:
+                best[0].close()
+            best = (b, ms, lanes)
+        else:
+            b.close()
+    b, batch_ms, lanes = best
+    L.mkf_launch_count(1)
+    batch_ms = timed(lambda: b.launch(cs), reps)
+    kernels = int(L.mkf_launch_count(0)) // (reps + max(1, a.warmup))
+    n = len(items)
+    res = {"workload": f"{n} MK-CKKS mult+relin+rescale+materialize products, k uniform over "
+                       "{2,4,8,16}, logN uniform over {14 (S14: 55b+7x40b, P 2x45b), "
+                       "15 (S15: 60b+15x50b, P 4x60b)}, level uniform over [1,L]",
+           "products": n,
+           "plain": {"value": n / (plain_ms / 1e3), "unit": "mult+relin ops/s", "ms": plain_ms},
+           "batched": {"value": n / (batch_ms / 1e3), "unit": "mult+relin ops/s", "ms": batch_ms,
+                       "lanes": lanes, "graph": True, "kernels_per_launch": kernels},
+           "batched_over_plain": plain_ms / batch_ms,
+           "autotune_lanes_ms": tried,
+           "mix": {f"k{k}": sum(1 for s in shapes if s[1] == k) for k in (2, 4, 8, 16)}}
+    b.close()
+    return res
 
 
 def ctypes_stream(s):
