@@ -213,6 +213,55 @@ uint64_t mkf_batch_kernels(const mkf_batch *batch);
 mkf_status mkf_mulrelin_batch(mkf_ctx *ctx, mkf_job *jobs, int n, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* serving loop                                                         */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference (which runs products serially on the
+ * caller's goroutine).  A server owns one device-memory pool for request
+ * scratch, allocated once, and `slots` streams.  Requests (mkf_job) are
+ * queued on submit and admitted in arrival order as soon as a slot is free
+ * and their scratch footprint (a dry run of the product) fits in the pool;
+ * a request that does not fit lets later, smaller ones pass, at most 32
+ * times, before it blocks admission until it fits.  Admitted requests run
+ * concurrently, each on its own slot stream, so requests that arrive while
+ * others are on the GPU overlap with them (continuous batching).  Nothing is
+ * allocated on the device after mkf_server_create. */
+typedef struct mkf_server mkf_server;
+typedef struct mkf_server_config {
+    int device;
+    size_t scratch_bytes; /* request scratch pool */
+    int slots;            /* requests in flight at most */
+    int queue_cap;        /* queued requests at most (submit: MKF_ERR_BUSY) */
+} mkf_server_config;
+typedef struct mkf_server_stats {
+    uint64_t submitted, completed, failed, rejected, cancelled;
+    double p50_ms, p99_ms, max_ms, mean_ms; /* submit -> result complete on the device */
+    double span_s;          /* first submit -> last completion */
+    size_t scratch_peak_bytes;
+    int inflight_peak;
+} mkf_server_stats;
+mkf_status mkf_server_create(const mkf_server_config *cfg, mkf_server **out);
+/* Device scratch bytes one job needs (the server's admission footprint). */
+mkf_status mkf_job_scratch(const mkf_job *job, size_t *bytes);
+/* Queues one product (handles must stay valid until it completes).
+ * Invalid jobs fail here with the single call's status; a job whose scratch
+ * exceeds the whole pool gives MKF_ERR_OOM; a full queue MKF_ERR_BUSY. */
+mkf_status mkf_server_submit(mkf_server *s, const mkf_job *job, uint64_t *ticket);
+/* Waits up to timeout_s (< 0: no limit) for a ticket; on completion returns
+ * MKF_OK with the job's own status and its latency, and forgets the ticket.
+ * MKF_ERR_TIMEOUT if it has not completed in time (the ticket stays valid). */
+mkf_status mkf_server_wait(mkf_server *s, uint64_t ticket, double timeout_s,
+                           mkf_status *job_status, double *latency_ms);
+/* Waits until nothing is queued or in flight (timeout_s < 0: no limit). */
+mkf_status mkf_server_drain(mkf_server *s, double timeout_s);
+/* Stops (paused != 0) or resumes admission; queued requests stay queued. */
+mkf_status mkf_server_pause(mkf_server *s, int paused);
+mkf_status mkf_server_stats_get(mkf_server *s, mkf_server_stats *out);
+mkf_status mkf_server_stats_reset(mkf_server *s);
+/* Cancels queued requests (MKF_ERR_CANCELLED), waits for the ones in
+ * flight, frees the pool and the streams. */
+void mkf_server_destroy(mkf_server *s);
+
+/* ------------------------------------------------------------------ */
 /* rescale and stage-level primitives                                   */
 /* ------------------------------------------------------------------ */
 /* Rescale by the last moduli while scale/q >= min_scale/2 (Lattigo

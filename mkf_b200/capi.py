@@ -67,6 +67,21 @@ class Job(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t),
+                ("slots", ctypes.c_int), ("queue_cap", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("span_s", ctypes.c_double), ("scratch_peak_bytes", ctypes.c_size_t),
+                ("inflight_peak", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -124,6 +139,15 @@ def lib():
         "mkf_batch_destroy": (None, [vp]),
         "mkf_batch_kernels": (ctypes.c_uint64, [vp]),
         "mkf_mulrelin_batch": (i, [vp, ctypes.POINTER(Job), i, vp]),
+        "mkf_server_create": (i, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+        "mkf_job_scratch": (i, [ctypes.POINTER(Job), ctypes.POINTER(sz)]),
+        "mkf_server_submit": (i, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]),
+        "mkf_server_wait": (i, [vp, ctypes.c_uint64, d, ctypes.POINTER(i), ctypes.POINTER(d)]),
+        "mkf_server_drain": (i, [vp, d]),
+        "mkf_server_pause": (i, [vp, i]),
+        "mkf_server_stats_get": (i, [vp, ctypes.POINTER(ServerStats)]),
+        "mkf_server_stats_reset": (i, [vp]),
+        "mkf_server_destroy": (None, [vp]),
         "mkf_profile_enable": (i, [vp, i]),
         "mkf_profile_kinds": (i, []),
         "mkf_profile_kind_name": (ctypes.c_char_p, [i]),

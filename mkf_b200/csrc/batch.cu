@@ -216,10 +216,7 @@ mkf_status mkf_mulrelin_batch(mkf_ctx *ctx, mkf_job *jobs, int n, void *stream) 
     mkf_status s = mkf_batch_create(ctx, jobs, n, std::min(std::max(n, 1), 8), 0, &b);
     if (s != MKF_OK) return s;
     s = mkf_batch_launch(b, stream);
-    // the plan's calls own KKLSS alignment temporaries: wait before freeing
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    cudaStreamSynchronize(st);
-    mkf_batch_destroy(b);
+    mkf_batch_destroy(b); // waits for the device before the lanes are reused
     return s;
 }
 

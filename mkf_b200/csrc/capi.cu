@@ -53,14 +53,6 @@ mkf_status status_of(const std::string &e) {
     return MKF_ERR_INVALID_ARG;
 }
 
-Call::~Call() {
-    if (!temps.empty()) {
-        cudaSetDevice(ctx->c.device);
-        cudaDeviceSynchronize();
-        for (mkf_ct *t : temps) mkf_ct_destroy(t);
-    }
-}
-
 mkf_status call_scratch(Call &call, size_t *words) {
     Arena dry;
     dry.dry = true;
@@ -68,6 +60,15 @@ mkf_status call_scratch(Call &call, size_t *words) {
     if (!e.empty()) return fail(call.ctx, status_of(e), e);
     *words = dry.peak;
     return MKF_OK;
+}
+
+mkf_status run_call_arena(Call &call, cudaStream_t st, Arena &a) {
+    cudaSetDevice(call.ctx->c.device);
+    std::string e = call.body(a, st);
+    if (!e.empty()) return fail(call.ctx, status_of(e), e);
+    mkf_status s = cuda_check(call.ctx, "kernel launch");
+    if (s == MKF_OK && call.commit) call.commit();
+    return s;
 }
 
 mkf_status run_call(Call &call, cudaStream_t st) {
@@ -180,54 +181,49 @@ mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
                     "output must have " + std::to_string(k + 1) + " components at level " +
                         std::to_string(lout));
     call.ctx = ctx;
-    // operands whose party list differs from the union are copied into
-    // union-ordered temporaries (absent components are zero) on every issue
+    // operands whose party list differs from the union are copied, on every
+    // issue, into union-ordered scratch copies (absent components are zero)
     struct Align {
         const uint64_t *src = nullptr;
         long long src_cs = 0;
-        uint64_t *dst = nullptr;
         std::vector<int> pos; // union position of each source party component
+        bool needed = false;
     };
-    std::vector<Align> aligns;
+    Align al[2];
     Operand O[2];
     const long long w = (long long)(level + 1) * ctx->c.N;
     const mkf_ct *ops[2] = {op0, op1};
     for (int j = 0; j < 2; ++j) {
         const mkf_ct *op = ops[j];
-        if (op->ids == u) {
-            O[j] = Operand{op->d, op->cs(), op->ncomp, op->level};
-            continue;
-        }
-        mkf_ct *t = nullptr;
-        mkf_status s = mkf_ct_create(ctx, k + 1, level, 0, &t);
-        if (s != MKF_OK) return s;
-        call.temps.push_back(t);
-        Align al;
-        al.src = op->d;
-        al.src_cs = op->cs();
-        al.dst = t->d;
-        for (int32_t id : op->ids) al.pos.push_back((int)(std::find(u.begin(), u.end(), id) - u.begin()));
-        aligns.push_back(al);
-        O[j] = Operand{t->d, w, k + 1, level};
+        O[j] = Operand{op->d, op->cs(), op->ncomp, op->level};
+        if (op->ids == u) continue;
+        al[j].needed = true;
+        al[j].src = op->d;
+        al[j].src_cs = op->cs();
+        for (int32_t id : op->ids) al[j].pos.push_back((int)(std::find(u.begin(), u.end(), id) - u.begin()));
+        O[j] = Operand{nullptr, w, k + 1, level};
     }
-    const int N = ctx->c.N;
-    (void)N;
     const uint64_t *crs = ks->crs_u;
     uint64_t *od = out->d;
     const long long ocs = out->cs();
+    const Align A0 = al[0], A1 = al[1];
     const Operand O0 = O[0], O1 = O[1];
-    call.body = [ctx, bfv, k, level, O0, O1, kp, crs, nb, od, ocs, aligns, w](Arena &a, cudaStream_t st) {
-        if (!a.dry) {
-            for (const Align &al : aligns) {
-                cudaMemsetAsync(al.dst, 0, (size_t)(k + 1) * w * 8, st);
-                cudaMemcpyAsync(al.dst, al.src, w * 8, cudaMemcpyDeviceToDevice, st);
-                for (size_t i = 0; i < al.pos.size(); ++i)
-                    cudaMemcpyAsync(al.dst + (long long)(al.pos[i] + 1) * w,
-                                    al.src + (long long)(i + 1) * al.src_cs, w * 8,
-                                    cudaMemcpyDeviceToDevice, st);
-            }
+    call.body = [ctx, bfv, k, level, O0, O1, A0, A1, kp, crs, nb, od, ocs, w](Arena &a, cudaStream_t st) {
+        Operand o[2] = {O0, O1};
+        const Align *aa[2] = {&A0, &A1};
+        for (int j = 0; j < 2; ++j) {
+            if (!aa[j]->needed) continue;
+            uint64_t *t = a.take((size_t)(k + 1) * w);
+            o[j].data = t;
+            if (a.dry) continue;
+            cudaMemsetAsync(t, 0, (size_t)(k + 1) * w * 8, st);
+            cudaMemcpyAsync(t, aa[j]->src, w * 8, cudaMemcpyDeviceToDevice, st);
+            for (size_t i = 0; i < aa[j]->pos.size(); ++i)
+                cudaMemcpyAsync(t + (long long)(aa[j]->pos[i] + 1) * w,
+                                aa[j]->src + (long long)(i + 1) * aa[j]->src_cs, w * 8,
+                                cudaMemcpyDeviceToDevice, st);
         }
-        return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, O0, O1, kp, crs, nb, od, ocs);
+        return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, o[0], o[1], kp, crs, nb, od, ocs);
     };
     call.commit = [out, u, scale]() {
         out->ids = u;

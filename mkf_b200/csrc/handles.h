@@ -61,22 +61,15 @@ mkf_status cuda_check(mkf_ctx *ctx, const char *where);
 Workspace *workspace(mkf_ctx *ctx, cudaStream_t st);
 mkf_status status_of(const std::string &e);
 
-// A validated mult+relin: body(arena, stream) issues its kernels, commit()
-// writes the output's metadata (scale, party ids, domain) once it succeeded.
-// temps are operand copies aligned to the KKLSS union party list, owned by
-// the call and refreshed by body on every issue.
+// A validated mult+relin: body(arena, stream) issues its kernels (all its
+// temporaries, including KKLSS operands re-ordered to the union party list,
+// come from the arena), commit() writes the output's metadata (scale, party
+// ids, domain) once it succeeded.
 struct Call {
     mkf_ctx *ctx = nullptr;
     std::function<std::string(Arena &, cudaStream_t)> body;
     std::function<void()> commit;
-    std::vector<mkf_ct *> temps;
     double cost = 0; // relative device work, for load balancing
-    Call() = default;
-    Call(const Call &) = delete;
-    Call &operator=(const Call &) = delete;
-    Call(Call &&) = default;
-    Call &operator=(Call &&) = default;
-    ~Call();
 };
 
 mkf_status prepare_mkf(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
@@ -87,6 +80,8 @@ mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
 mkf_status call_scratch(Call &call, size_t *words);
 // Issues the call on st, growing st's workspace first unless st is capturing.
 mkf_status run_call(Call &call, cudaStream_t st);
+// Issues the call on st with caller-provided scratch (at least call_scratch).
+mkf_status run_call_arena(Call &call, cudaStream_t st, Arena &a);
 // Lane i of the context's batch streams (created on first use), or nullptr.
 cudaStream_t ctx_lane(mkf_ctx *ctx, int i);
 

@@ -343,6 +343,94 @@ class Batch:
             pass
 
 
+def make_job(job) -> "capi.Job":
+    """struct mkf_job from ("mkf", MKFEvaluator, left, right, out, rescale,
+    materialize) or ("kklss", RelinearizationKeySet, op0, op1, out)."""
+    j = capi.Job()
+    if job[0] == "mkf":
+        _, ev_, left, right, out, rescale, materialize = job
+        j.kind, j.mkf_keys = capi.JOB_MKF, ev_.keys.handle
+        j.flags = (capi.FLAG_RESCALE if rescale else 0) | (capi.FLAG_MATERIALIZE if materialize else 0)
+    else:
+        _, rlk, left, right, out = job
+        j.kind, j.kklss_keys = capi.JOB_KKLSS, rlk.handle
+    j.a, j.b, j.out = left.handle, right.handle, out.handle
+    return j
+
+
+def job_scratch_bytes(job) -> int:
+    j = make_job(job)
+    n = ctypes.c_size_t()
+    st = capi.lib().mkf_job_scratch(ctypes.byref(j), ctypes.byref(n))
+    capi.check(job[2].params.handle, st)
+    return int(n.value)
+
+
+class Server:
+    """The serving loop (mkf_server_*): submit products as they arrive,
+    wait for tickets, read p50/p99 latency and throughput."""
+
+    def __init__(self, device: int = 0, scratch_bytes: int = 8 << 30, slots: int = 8,
+                 queue_cap: int = 4096):
+        cfg = capi.ServerConfig(device, scratch_bytes, slots, queue_cap)
+        h = ctypes.c_void_p()
+        st = capi.lib().mkf_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != capi.OK:
+            raise capi.MKFError(st, "mkf_server_create failed")
+        self.handle = h
+        self._live = {}
+
+    def submit(self, job) -> int:
+        """Queues one job; returns its ticket or raises MKFError (BUSY, OOM,
+        validation errors with the job's own status)."""
+        j = make_job(job)
+        t = ctypes.c_uint64()
+        st = capi.lib().mkf_server_submit(self.handle, ctypes.byref(j), ctypes.byref(t))
+        if st != capi.OK:
+            capi.check(job[2].params.handle, st)
+        self._live[t.value] = job  # keep the handles alive until waited
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0):
+        """Returns (job status, latency ms); raises MKFError(TIMEOUT) when the
+        ticket has not completed within timeout_s."""
+        js, lat = ctypes.c_int(), ctypes.c_double()
+        st = capi.lib().mkf_server_wait(self.handle, ticket, float(timeout_s), ctypes.byref(js),
+                                        ctypes.byref(lat))
+        if st != capi.OK:
+            raise capi.MKFError(st, f"ticket {ticket}")
+        self._live.pop(ticket, None)
+        return int(js.value), float(lat.value)
+
+    def drain(self, timeout_s: float = -1.0):
+        st = capi.lib().mkf_server_drain(self.handle, float(timeout_s))
+        if st != capi.OK:
+            raise capi.MKFError(st, "drain")
+
+    def pause(self, paused: bool = True):
+        capi.lib().mkf_server_pause(self.handle, int(paused))
+
+    def stats(self) -> dict:
+        s = capi.ServerStats()
+        capi.lib().mkf_server_stats_get(self.handle, ctypes.byref(s))
+        return {f: getattr(s, f) for f, _ in capi.ServerStats._fields_}
+
+    def reset_stats(self):
+        capi.lib().mkf_server_stats_reset(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            capi.lib().mkf_server_destroy(self.handle)
+            self.handle = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # stage-level primitives ------------------------------------------------------
 
 def ntt(params: Parameters, arr: np.ndarray, basis: str = "Q", first: int = 0, inverse=False):
