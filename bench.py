@@ -51,6 +51,13 @@ def parse():
                     help="products in the mixed batch (k in {2,4,8,16}, logN in {14,15}, "
                          "level uniform over [1,L]); 0 skips it")
     ap.add_argument("--lanes", default="4,8,16", help="lane counts the batch autotuner tries")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="length of the open-loop Poisson trace; 0 skips serving")
+    ap.add_argument("--serve-rate", type=float, default=1000.0,
+                    help="offered load (req/s); capped at 0.8 x the measured capacity")
+    ap.add_argument("--serve-parties16", type=int, default=16,
+                    help="party-pool size of the logN=16 rings (64 for the full pool)")
+    ap.add_argument("--serve-templates", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -431,6 +438,7 @@ def run_gpu(a):
                "d2h_bytes_per_step": a.batch * words_out * 8}
 
     mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
+    serve = run_serve(a, local, rank) if a.serve_seconds > 0 else None
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -456,6 +464,7 @@ def run_gpu(a):
             "gpu_launches": launches,
             "roofline": roofline,
             "batched_mix": mix,
+            "serving": serve,
             "kernels": kinds,
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -561,6 +570,110 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
            "mix": {f"k{k}": sum(1 for s in shapes if s[1] == k) for k in (2, 4, 8, 16)}}
     b.close()
     return res
+
+
+def run_serve(a, local, rank):
+    """Open-loop serving trace through the serving loop (mkf_server_*): KKLSS
+    mult+relin requests, scheme 50/50 CKKS/BFV, ring uniform over logN
+    {14,15,16}, k uniform over {2..16} parties drawn from a per-ring key pool
+    (64 parties at logN 14/15, `--serve-parties16` at 16), level uniform.
+    Per-party relinearization keys are distinct HBM buffers.  Requests are
+    drawn from `--serve-templates` prepared operand sets.  First a closed burst
+    measures capacity; then Poisson arrivals at min(rate, 0.8 x capacity)."""
+    import time
+    from mkf_b200 import capi, params
+    from mkf_b200 import evaluator as ev
+    g = np.random.Generator(np.random.PCG64(999 + rank))
+    rings = []
+    key_bytes = 0
+    for scheme in ("ckks", "bfv"):
+        for name, npart in (("S14", 64), ("S15", 64), ("S16", a.serve_parties16)):
+            lit = params.get(scheme, name)
+            P = ev.Parameters(lit, scheme, device=local)
+            qmin = min(min(lit.q), min(lit.p), min(lit.q_mul) if lit.q_mul else 1 << 62)
+            kind = capi.KEY_KKLSS_RLK if scheme == "ckks" else capi.KEY_KKLSS_BFV_RLK
+            img = g.integers(0, qmin, size=P.key_words(kind), dtype=np.uint64)
+            rlk = ev.RelinearizationKeySet(P, g.integers(0, qmin, size=P.key_words(capi.KEY_GADGET),
+                                                          dtype=np.uint64))
+            for pid in range(npart):
+                rlk.AddRelinearizationKey(pid, img)
+            key_bytes += 8 * npart * img.size
+            N, nq = lit.n, len(lit.q)
+            buf = g.integers(0, qmin, size=17 * nq * N, dtype=np.uint64)
+            rings.append((scheme, name, lit, P, rlk, npart, buf))
+    E = {}
+    templates = []
+    for _ in range(a.serve_templates):
+        scheme, name, lit, P, rlk, npart, buf = rings[int(g.integers(len(rings)))]
+        k = int(g.integers(2, 17))
+        level = int(g.integers(1, lit.max_level + 1)) if scheme == "ckks" else lit.max_level
+        ids = [int(x) for x in g.choice(npart, size=k, replace=False)]
+        words = (k + 1) * (level + 1) * lit.n
+        ops = []
+        for _ in range(2):
+            c = ev.Ciphertext(P, k + 1, level, False, ids=ids, scale=lit.scale if scheme == "ckks" else None)
+            c.upload(buf[:words].reshape(k + 1, level + 1, lit.n))
+            ops.append(c)
+        ev_ = E.setdefault(id(P), ev.Evaluator(P))
+        ref_level = level - 1 if scheme == "ckks" else level
+        outs = [ev.Ciphertext(P, k + 1, ref_level, False) for _ in range(2)]
+        templates.append([("kklss", rlk, ops[0], ops[1], o) for o in outs])
+    need = max(ev.job_scratch_bytes(t[0]) for t in templates)
+    slots = 8
+    pool = int(min(max(need * 3, 8 << 30), 40 << 30))
+    srv = ev.Server(device=local, scratch_bytes=pool, slots=slots, queue_cap=4096)
+    # closed burst: capacity
+    burst = [templates[i % len(templates)][i % 2] for i in range(2 * len(templates))]
+    for j in burst[: len(templates)]:
+        srv.submit(j)
+    srv.drain()
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    for j in burst:
+        srv.submit(j)
+    srv.drain()
+    cap_s = time.perf_counter() - t0
+    capacity = len(burst) / cap_s
+    burst_stats = srv.stats()
+    srv.reset_stats()
+    # open loop
+    rate = min(a.serve_rate, 0.8 * capacity)
+    n_req = max(1, int(rate * a.serve_seconds))
+    gaps = g.exponential(1.0 / rate, size=n_req)
+    picks = g.integers(0, len(templates), size=n_req)
+    tickets, busy = [], 0
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i in range(n_req):
+        t_next += gaps[i]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        try:
+            tickets.append(srv.submit(templates[picks[i]][i % 2]))
+        except capi.MKFError as e:
+            if e.status != 8:
+                raise
+            busy += 1
+    srv.drain()
+    wall = time.perf_counter() - t_start
+    st = srv.stats()
+    srv.close()
+    return {"workload": "open-loop Poisson trace of KKLSS mult+relin requests: CKKS/BFV 50/50, "
+                        "logN uniform over {14,15,16} (S14/S15/S16 sets), k uniform over {2..16} "
+                        "from a per-ring party pool, level uniform (CKKS)",
+            "offered_req_s": rate, "requested_rate_req_s": a.serve_rate,
+            "seconds": a.serve_seconds, "requests": n_req, "busy_rejected": busy,
+            "throughput_req_s": st["completed"] / wall if wall > 0 else None,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+            "inflight_peak": st["inflight_peak"], "slots": slots,
+            "scratch_pool_gb": pool / 1e9, "scratch_peak_gb": st["scratch_peak_bytes"] / 1e9,
+            "key_pool_gb": key_bytes / 1e9,
+            "party_pool": {"logN14": 64, "logN15": 64, "logN16": a.serve_parties16},
+            "capacity_req_s": capacity,
+            "capacity_burst": {"requests": len(burst), "p50_ms": burst_stats["p50_ms"],
+                               "p99_ms": burst_stats["p99_ms"]},
+            "latency": "submit -> result complete on the device (host callback)"}
 
 
 def ctypes_stream(s):
