@@ -153,6 +153,33 @@ enum {
 mkf_status mkf_mkf_mulrelin(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
                             const mkf_mkf_keyset *ks, int flags, mkf_ct *out, void *stream);
 
+/* MKF fold alone (fold, software/mkf/mkf_cpu/common.go:109-126; the paper
+ * adapter's foldCarrierToAggregate, true_mkf_ckks_adapter.go:190-203): the
+ * (k+1)-component k-party ciphertext `in` (CKKS: NTT domain; BFV:
+ * coefficient domain) becomes the compact (c0, Gamma) pair under the
+ * aggregate secret.  `out`: 2 components at in's level; scale kept. */
+mkf_status mkf_mkf_fold(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *ks, mkf_ct *out,
+                        void *stream);
+/* Repeated-Gamma materialization (materialize, common.go:128-139;
+ * materializeAggregate, true_mkf_ckks_adapter.go:205-222): the compact
+ * (c0, Gamma) pair becomes c0 followed by Gamma once per party; `out` has
+ * the parties + 1 components at the compact ciphertext's level. */
+mkf_status mkf_mkf_materialize(mkf_ctx *ctx, const mkf_ct *compact, mkf_ct *out, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* component-wise public operations on (n+1)-component carriers          */
+/* ------------------------------------------------------------------ */
+/* The linear operations the paper adapter leaves to Lattigo's evaluator and
+ * its public MulNew (true_mkf_ckks_adapter.go:80-127), applied to every
+ * component: out = a + b or a - b (same component count, party ids, domain
+ * and scale; level = the lower of the two), or out = ct * pt for a public
+ * plaintext `pt` (one component, NTT domain like ct; scale multiplies).
+ * `out` must have a's component count at the output level. */
+mkf_status mkf_add(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream);
+mkf_status mkf_sub(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream);
+mkf_status mkf_mul_plain(mkf_ctx *ctx, const mkf_ct *ct, const mkf_ct *pt, mkf_ct *out,
+                         void *stream);
+
 /* ------------------------------------------------------------------ */
 /* KKLSS per-party-key construction                                     */
 /* ------------------------------------------------------------------ */

@@ -1,0 +1,118 @@
+"""The paper-facing (n+1)-component interface over the GPU path.
+
+Mirrors paperMKFLattigoAdapter (software/mkf/mkf_cpu/true_mkf_ckks_adapter.go:
+13-252) and paperMKFCKKSEvaluator (true_mkf_ckks.go:227-304): a k-party
+MK-CKKS ciphertext is carried as c0 plus one component per party, all in the
+NTT domain, so that code written against the carrier interface (packing,
+linear layers, products) runs unchanged.
+
+* MulRelinNew / MulRelin: the MKF product without rescale, output
+  materialized to n+1 components (true_mkf_ckks.go:253-304);
+* MulNew / Mul: a public NTT-domain plaintext applied to every component
+  (adapter MulNew, :80-127);
+* AddNew / SubNew / Add / Sub: component-wise linear operations (the
+  embedded Lattigo evaluator's job in the reference);
+* Rescale / RescaleNew (true_mkf_ckks.go RescaleNew; Lattigo Rescale);
+* FoldToAggregate / MaterializeAggregate (foldCarrierToAggregate,
+  materializeAggregate, :190-222).
+
+Rotations and polynomial evaluation (RotateNew, EvaluatePoly) need Galois
+keys and the polynomial evaluator, which this library does not provide;
+they raise NotImplementedError.  The collective refresh protocol is out of
+scope.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+from . import capi
+from .evaluator import Ciphertext, Evaluator, MKFEvaluator, MKFKeySet, Parameters
+
+
+class PaperMKFAdapter:
+    def __init__(self, params: Parameters, keys: MKFKeySet):
+        if params.scheme != "ckks":
+            raise ValueError("the paper interface is MK-CKKS")
+        self.params, self.keys = params, keys
+        self.parties = keys.k
+        self._mkf = MKFEvaluator(params, keys)
+        self._ev = Evaluator(params)
+
+    # carriers -------------------------------------------------------------
+    def NewCiphertext(self, level: int, scale: Optional[float] = None) -> Ciphertext:
+        return Ciphertext(self.params, self.parties + 1, level, True,
+                          scale=self.params.Scale() if scale is None else scale)
+
+    def _check_carrier(self, ct: Ciphertext, what: str):
+        if ct.n_comp != self.parties + 1:
+            raise ValueError(f"{what}: expected a {self.parties + 1}-component carrier, got {ct.n_comp}")
+
+    # products -------------------------------------------------------------
+    def MulRelinNew(self, left: Ciphertext, right: Ciphertext) -> Ciphertext:
+        self._check_carrier(left, "MulRelin")
+        self._check_carrier(right, "MulRelin")
+        return self._mkf.MulRelinNew(left, right, rescale=False, materialize=True)
+
+    def MulRelin(self, left: Ciphertext, right: Ciphertext, out: Ciphertext):
+        self._check_carrier(out, "MulRelin output")
+        self._mkf.MulRelin(left, right, out, rescale=False, materialize=True)
+
+    def MulNew(self, carrier: Ciphertext, public: Ciphertext) -> Ciphertext:
+        self._check_carrier(carrier, "Mul")
+        out = Ciphertext(self.params, carrier.n_comp, min(carrier.Level(), public.Level()), True)
+        self.Mul(carrier, public, out)
+        return out
+
+    def Mul(self, carrier: Ciphertext, public: Ciphertext, out: Ciphertext):
+        capi.check(self.params.handle, capi.lib().mkf_mul_plain(
+            self.params.handle, carrier.handle, public.handle, out.handle, None))
+
+    # linear -----------------------------------------------------------------
+    def _ew(self, fn, a, b, out):
+        capi.check(self.params.handle, fn(self.params.handle, a.handle, b.handle, out.handle, None))
+
+    def AddNew(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
+        out = Ciphertext(self.params, a.n_comp, min(a.Level(), b.Level()), True)
+        self._ew(capi.lib().mkf_add, a, b, out)
+        return out
+
+    def SubNew(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
+        out = Ciphertext(self.params, a.n_comp, min(a.Level(), b.Level()), True)
+        self._ew(capi.lib().mkf_sub, a, b, out)
+        return out
+
+    def Add(self, a, b, out):
+        self._ew(capi.lib().mkf_add, a, b, out)
+
+    def Sub(self, a, b, out):
+        self._ew(capi.lib().mkf_sub, a, b, out)
+
+    # rescale ----------------------------------------------------------------
+    def RescaleNew(self, ct: Ciphertext, minScale: Optional[float] = None) -> Ciphertext:
+        return self._ev.RescaleNew(ct, self.params.Scale() if minScale is None else minScale)
+
+    def Rescale(self, ct: Ciphertext, minScale: float, out: Ciphertext):
+        self._ev.Rescale(ct, minScale, out)
+
+    # aggregate form ---------------------------------------------------------
+    def FoldToAggregate(self, carrier: Ciphertext) -> Ciphertext:
+        """The compact (c0, Gamma) pair under the aggregate secret."""
+        self._check_carrier(carrier, "fold")
+        out = Ciphertext(self.params, 2, carrier.Level(), True)
+        capi.check(self.params.handle, capi.lib().mkf_mkf_fold(
+            self.params.handle, carrier.handle, self.keys.handle, out.handle, None))
+        return out
+
+    def MaterializeAggregate(self, compact: Ciphertext) -> Ciphertext:
+        """c0, then Gamma once per party."""
+        out = Ciphertext(self.params, self.parties + 1, compact.Level(), True)
+        capi.check(self.params.handle, capi.lib().mkf_mkf_materialize(
+            self.params.handle, compact.handle, out.handle, None))
+        return out
+
+    # not provided -----------------------------------------------------------
+    def RotateNew(self, ct, rotation):
+        raise NotImplementedError("rotations need Galois keys, which this library does not provide")
+
+    def EvaluatePoly(self, ct, polynomial, targetScale):
+        raise NotImplementedError("polynomial evaluation is not provided by this library")

@@ -139,6 +139,11 @@ def lib():
         "mkf_batch_destroy": (None, [vp]),
         "mkf_batch_kernels": (ctypes.c_uint64, [vp]),
         "mkf_mulrelin_batch": (i, [vp, ctypes.POINTER(Job), i, vp]),
+        "mkf_mkf_fold": (i, [vp, vp, vp, vp, vp]),
+        "mkf_mkf_materialize": (i, [vp, vp, vp, vp]),
+        "mkf_add": (i, [vp, vp, vp, vp, vp]),
+        "mkf_sub": (i, [vp, vp, vp, vp, vp]),
+        "mkf_mul_plain": (i, [vp, vp, vp, vp, vp]),
         "mkf_server_create": (i, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "mkf_job_scratch": (i, [ctypes.POINTER(Job), ctypes.POINTER(sz)]),
         "mkf_server_submit": (i, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]),

@@ -528,6 +528,105 @@ mkf_status mkf_mkf_mulrelin(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *righ
     return run_call(call, pick(ctx, stream));
 }
 
+mkf_status mkf_mkf_fold(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *ks, mkf_ct *out,
+                        void *stream) {
+    if (!ctx || !in || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (ks->ctx != ctx || in->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const int k = ks->k;
+    const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
+    if (in->ncomp != k + 1) return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
+    if (out->ncomp != 2 || out->level != in->level)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have 2 components at level " + std::to_string(in->level));
+    if ((bool)in->is_ntt == bfv)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    bfv ? "MKF BFV operands must be in the coefficient domain"
+                        : "MKF CKKS operands must be in the NTT domain");
+    const Operand I{in->d, in->cs(), in->ncomp, in->level};
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) kp.p[i] = ks->fold[i];
+    cudaStream_t st = pick(ctx, stream);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return mkf_fold(ctx->c, a, st, bfv ? kBFV : kCKKS, k, in->level, I, kp, out->d, out->cs());
+    });
+    if (s == MKF_OK) {
+        out->scale = in->scale;
+        out->is_ntt = in->is_ntt;
+        out->ids = {in->ids.empty() ? 0 : in->ids[0]};
+    }
+    return s;
+}
+
+mkf_status mkf_mkf_materialize(mkf_ctx *ctx, const mkf_ct *compact, mkf_ct *out, void *stream) {
+    if (!ctx || !compact || !out) return MKF_ERR_INVALID_ARG;
+    if (compact->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    if (compact->ncomp != 2) return fail(ctx, MKF_ERR_INVALID_ARG, "compact ciphertext must have 2 components");
+    if (out->ncomp < 2 || out->level != compact->level)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have at least 2 components at level " + std::to_string(compact->level));
+    cudaSetDevice(ctx->c.device);
+    cudaStream_t st = pick(ctx, stream);
+    const long long w = compact->cs();
+    cudaMemcpyAsync(out->d, compact->d, w * 8, cudaMemcpyDeviceToDevice, st);
+    launch_replicate(compact->d + w, out->d + out->cs(), w, out->ncomp - 1, out->cs(), st);
+    mkf_status s = cuda_check(ctx, "materialize");
+    if (s == MKF_OK) {
+        out->scale = compact->scale;
+        out->is_ntt = compact->is_ntt;
+    }
+    return s;
+}
+
+static mkf_status ew_entry(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, int op,
+                           void *stream) {
+    if (!ctx || !a || !b || !out) return MKF_ERR_INVALID_ARG;
+    if (a->ctx != ctx || b->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    const int level = std::min(a->level, b->level);
+    if (a->is_ntt != b->is_ntt) return fail(ctx, MKF_ERR_INVALID_ARG, "operands are in different domains");
+    double scale = a->scale;
+    if (op == kEwMul) {
+        if (b->ncomp != 1) return fail(ctx, MKF_ERR_INVALID_ARG, "the public operand must have 1 component");
+        if (!a->is_ntt) return fail(ctx, MKF_ERR_INVALID_ARG, "public products need NTT-domain operands");
+        scale = a->scale * b->scale;
+    } else {
+        if (a->ncomp != b->ncomp || a->ids != b->ids)
+            return fail(ctx, MKF_ERR_INVALID_ARG, "operands have different components or party ids");
+        const double d = a->scale - b->scale;
+        if (d > 1e-9 * a->scale || -d > 1e-9 * a->scale)
+            return fail(ctx, MKF_ERR_INVALID_ARG, "operands have different scales");
+    }
+    if (out->ncomp != a->ncomp || out->level != level)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(a->ncomp) + " components at level " +
+                        std::to_string(level));
+    cudaSetDevice(ctx->c.device);
+    cudaStream_t st = pick(ctx, stream);
+    launch_ew_binary(ctx->c, a->d, a->cs(), b->d, op == kEwMul ? 0 : b->cs(), out->d, out->cs(),
+                     a->ncomp, level + 1, qmap(level + 1), op, st);
+    mkf_status s = cuda_check(ctx, "elementwise");
+    if (s == MKF_OK) {
+        out->scale = scale;
+        out->is_ntt = a->is_ntt;
+        out->ids = a->ids;
+    }
+    return s;
+}
+
+mkf_status mkf_add(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream) {
+    return ew_entry(ctx, a, b, out, kEwAdd, stream);
+}
+mkf_status mkf_sub(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream) {
+    return ew_entry(ctx, a, b, out, kEwSub, stream);
+}
+mkf_status mkf_mul_plain(mkf_ctx *ctx, const mkf_ct *ct, const mkf_ct *pt, mkf_ct *out,
+                         void *stream) {
+    return ew_entry(ctx, ct, pt, out, kEwMul, stream);
+}
+
 mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out) {
     if (!ctx || !crs_u || !out) return MKF_ERR_INVALID_ARG;
     if (crs_u->kind != MKF_KEY_GADGET || crs_u->ctx != ctx)

@@ -109,6 +109,113 @@ void fill_ones(uint8_t *p, int n, cudaStream_t st) { cudaMemsetAsync(p, 1, n, st
 // ---------------------------------------------------------------------------
 // MKF
 // ---------------------------------------------------------------------------
+// Scratch of fold_sides (words), taken from the arena in this order.
+struct FoldScratch {
+    uint64_t *coeff = nullptr, *dig = nullptr, *acc = nullptr, *tmp = nullptr, *dscr = nullptr;
+};
+
+static FoldScratch take_fold_scratch(const Context &c, Arena &ar, bool bfv, int k, int level,
+                                     int nops) {
+    const int L1 = level + 1, beta = c.beta_of(level, 1);
+    const long long poly = (long long)L1 * c.N, qp = (long long)(L1 + c.nP) * c.N, kk = k;
+    FoldScratch f;
+    f.coeff = bfv ? nullptr : ar.take(nops * kk * poly);
+    f.dig = ar.take(nops * kk * beta * qp);
+    f.acc = ar.take(2 * nops * kk * qp);
+    f.tmp = ar.take(2 * nops * poly);
+    f.dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, nops * k));
+    return f;
+}
+
+// MKF fold of nops operands (fold, common.go:109-126):
+//   F[s][0] = C0_s + sum_i switchOne(c_{s,i}, Fold_i)[0],
+//   F[s][1] =        sum_i switchOne(c_{s,i}, Fold_i)[1],
+// F laid out [nops][2][L1][N] (CKKS: NTT domain; BFV: coefficient domain).
+// Every component of every operand is decomposed once; each fold key is read
+// once for all operands; each party's P part is lifted exactly (ModUp per
+// accumulator, as the reference's per-key ModDown does), the lifts are
+// summed mod q and transformed once per output, which equals the sum of the
+// per-party ModDowns exactly because NTT and P^-1 are linear mod q.
+static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int level,
+                       const Operand *ops, int nops, const KeyPtrs &fold, const FoldScratch &f,
+                       uint64_t *F) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1;
+    const int beta = c.beta_of(level, 1);
+    const long long poly = (long long)L1 * N, qp = (long long)(L1 + nP) * N, kk = k;
+    // 1. gadget decomposition of every party component
+    if (!bfv) {
+        OwnNtt own;
+        for (int s = 0; s < nops; ++s) {
+            d2d2(f.coeff + s * kk * poly, poly, ops[s].data + ops[s].cs, ops[s].cs, poly, k, st);
+            own.p[s] = ops[s].data + ops[s].cs;
+            own.pstride[s] = ops[s].cs;
+        }
+        own.split = k;
+        ntt_inverse(c, lsq(f.coeff, poly, L1), nops * k, st);
+        decompose_ntt(c, f.coeff, poly, 0, level, 1, beta, f.dig, nops * k, f.dscr, st, &own);
+    } else {
+        for (int s = 0; s < nops; ++s)
+            decompose_ntt(c, ops[s].data + ops[s].cs, ops[s].cs, 0, level, 1, beta,
+                          f.dig + s * kk * beta * qp, k, f.dscr, st);
+    }
+    // 2. fold key inner products: each key read once for every operand
+    IpArgs ip;
+    ip.A = f.dig;
+    ip.a_tstride = qp;
+    ip.a_gstride = beta * qp;
+    ip.a_istride = kk * beta * qp;
+    ip.use_bptr = 1;
+    for (int i = 0; i < k; ++i) ip.bptr[i] = fold.p[i];
+    ip.b_tstride = 2LL * (nQ + nP) * N;
+    ip.b_ostride = (long long)(nQ + nP) * N;
+    ip.b_qlimbs = nQ;
+    ip.out = f.acc;
+    ip.out_gstride = 2 * nops * qp;
+    ip.out_istride = 2 * qp;
+    ip.out_ostride = qp;
+    ip.nterms = beta;
+    ip.nin = nops;
+    ip.nout = 2;
+    ip.groups = k;
+    ip.L1 = L1;
+    ip.nP = nP;
+    launch_ip(c, ip, st);
+    // 3. ModDown summed over parties, then the fold
+    if (!bfv)
+        ntt_inverse(c, lsp_of_qp(c, f.acc, qp, L1), 2 * nops * k, st);
+    else
+        ntt_inverse(c, lsqp(c, f.acc, qp, L1), 2 * nops * k, st);
+    launch_modup_sum(c, c.p_to_q, f.acc + (long long)L1 * N, qp, 2 * nops * qp, k, f.tmp, poly, 0,
+                     L1, qmap(L1), 2 * nops, st);
+    if (!bfv) ntt_forward(c, lsq(f.tmp, poly, L1), 2 * nops, st);
+    for (int s = 0; s < nops; ++s) {
+        d2d2(F + 2 * s * poly, poly, ops[s].data, ops[s].cs, poly, 1, st);
+        cudaMemsetAsync(F + (2 * s + 1) * poly, 0, poly * 8, st);
+    }
+    CombineSpec cs = pdown(c, f.acc, qp, f.tmp, poly, F, poly, 1);
+    cs.x_tstride = 2 * nops * qp;
+    cs.terms = k;
+    cs.y_single = 1;
+    launch_moddown_combine(c, cs, L1, qmap(L1), 2 * nops, st);
+}
+
+std::string mkf_fold(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k, int level,
+                     const Operand &in, const KeyPtrs &fold, uint64_t *out, long long out_cs) {
+    const bool bfv = scheme == kBFV;
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (level < 0 || level >= c.nQ) return "level out of range";
+    if (c.nP > 8) return "at most 8 special primes are supported";
+    if (in.ncomp < k + 1) return "operand has fewer than k+1 components";
+    if (in.level < level) return "operand level below the fold level";
+    const long long poly = (long long)(level + 1) * c.N;
+    FoldScratch f = take_fold_scratch(c, ar, bfv, k, level, 1);
+    uint64_t *F = ar.take(2 * poly);
+    if (ar.dry) return "";
+    fold_sides(c, st, bfv, k, level, &in, 1, fold, f, F);
+    d2d2(out, out_cs, F, poly, poly, 2, st);
+    return "";
+}
+
 std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
                          int level, const Operand &left, const Operand &right,
                          const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,
@@ -127,12 +234,8 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     const long long poly = (long long)L1 * N, qp = (long long)NQP * N;
     const int nR = nQ + c.nQM;
     const long long rp = (long long)nR * N;
-    const long long kk = k;
 
-    uint64_t *coeff = bfv ? nullptr : ar.take(2 * kk * poly);
-    uint64_t *dig = ar.take(2 * kk * beta * qp);
-    uint64_t *acc = ar.take(4 * kk * qp);
-    uint64_t *tmp = ar.take(4 * poly);
+    FoldScratch fs = take_fold_scratch(c, ar, bfv, k, level, 2);
     uint64_t *F = ar.take(4 * poly);
     uint64_t *mu = ar.take(3 * poly);
     uint64_t *rcoef = bfv ? nullptr : ar.take(poly);
@@ -146,73 +249,12 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     uint64_t *yq = bfv ? ar.take(3 * poly) : nullptr;
     uint64_t *last = bfv ? nullptr : ar.take(2LL * N);
     uint64_t *tr = bfv ? nullptr : ar.take(2 * poly);
-    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, 2 * k));
+    uint64_t *dscr = fs.dscr;
     if (ar.dry) return "";
 
-    // 1. gadget decomposition of every component of both operands
-    if (!bfv) {
-        d2d2(coeff, poly, left.data + left.cs, left.cs, poly, k, st);
-        d2d2(coeff + kk * poly, poly, right.data + right.cs, right.cs, poly, k, st);
-        ntt_inverse(c, lsq(coeff, poly, L1), 2 * k, st);
-        OwnNtt own;
-        own.p[0] = left.data + left.cs;
-        own.p[1] = right.data + right.cs;
-        own.pstride[0] = left.cs;
-        own.pstride[1] = right.cs;
-        own.split = k;
-        decompose_ntt(c, coeff, poly, 0, level, 1, beta, dig, 2 * k, dscr, st, &own);
-    } else {
-        decompose_ntt(c, left.data + left.cs, left.cs, 0, level, 1, beta, dig, k, dscr, st);
-        decompose_ntt(c, right.data + right.cs, right.cs, 0, level, 1, beta, dig + kk * beta * qp, k,
-                      dscr, st);
-    }
-
-    // 2. fold key inner products: each key read once for both operands
-    IpArgs ip;
-    ip.A = dig;
-    ip.a_tstride = qp;
-    ip.a_gstride = beta * qp;
-    ip.a_istride = kk * beta * qp;
-    ip.use_bptr = 1;
-    for (int i = 0; i < k; ++i) ip.bptr[i] = fold.p[i];
-    ip.b_tstride = 2LL * (nQ + nP) * N;
-    ip.b_ostride = (long long)(nQ + nP) * N;
-    ip.b_qlimbs = nQ;
-    ip.out = acc;
-    ip.out_gstride = 4 * qp;
-    ip.out_istride = 2 * qp;
-    ip.out_ostride = qp;
-    ip.nterms = beta;
-    ip.nin = 2;
-    ip.nout = 2;
-    ip.groups = k;
-    ip.L1 = L1;
-    ip.nP = nP;
-    launch_ip(c, ip, st);
-
-    // 3. ModDown and fold: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1.
-    // Each party's P part is lifted exactly (ModUp per accumulator, as the
-    // reference's per-key ModDown does); the lifts are then summed mod q and
-    // transformed once per output, which equals the sum of the per-party
-    // ModDowns exactly because both NTT and P^-1 are linear mod q.
-    if (!bfv)
-        ntt_inverse(c, lsp_of_qp(c, acc, qp, L1), 4 * k, st);
-    else
-        ntt_inverse(c, lsqp(c, acc, qp, L1), 4 * k, st);
-    launch_modup_sum(c, c.p_to_q, acc + (long long)L1 * N, qp, 4 * qp, k, tmp, poly, 0, L1,
-                     qmap(L1), 4, st);
-    if (!bfv) ntt_forward(c, lsq(tmp, poly, L1), 4, st);
-    d2d2(F, 2 * poly, left.data, left.cs, poly, 1, st);
-    d2d2(F + 2 * poly, 2 * poly, right.data, right.cs, poly, 1, st);
-    cudaMemsetAsync(F + poly, 0, poly * 8, st);
-    cudaMemsetAsync(F + 3 * poly, 0, poly * 8, st);
-    {
-        CombineSpec s = pdown(c, acc, qp, tmp, poly, F, poly, 1);
-        s.x_tstride = 4 * qp;
-        s.terms = k;
-        s.y_single = 1;
-        launch_moddown_combine(c, s, L1, qmap(L1), 4, st);
-    }
+    // 1-3. fold both operands: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1
+    const Operand ops[2] = {left, right};
+    fold_sides(c, st, bfv, k, level, ops, 2, fold, fs, F);
 
     uint64_t *mu0 = mu, *mu1 = mu + poly, *mu2 = mu + 2 * poly;
     if (!bfv) {

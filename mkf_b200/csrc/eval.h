@@ -69,6 +69,12 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
                          const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,
                          uint64_t *out, long long out_cs);
 
+// MKF fold of one operand (common.go:109-126): out = (C0 + sum_i p0_i,
+// sum_i p1_i), the compact ciphertext under the aggregate secret, two
+// components at `level` (CKKS: NTT domain; BFV: coefficient domain).
+std::string mkf_fold(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k, int level,
+                     const Operand &in, const KeyPtrs &fold, uint64_t *out, long long out_cs);
+
 // KKLSS mult+relin with per-party (b, d, v) keys (software/kklss/mkckks/
 // evaluator.go:419-446,561-586; software/kklss/mkbfv/evaluator.go:85-152).
 // op0/op1: component 0 then one component per party of the union party set

@@ -502,6 +502,37 @@ void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModM
     add_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(acc, x, c.d_mods, mm, c.N);
 }
 
+// out_c = a_c (op) b_c over ncomp components of nl limbs (b_cs = 0: one b
+// polynomial for every component, as a public plaintext is applied)
+__global__ void ew_binary_kernel(const uint64_t *a, long long a_cs, const uint64_t *b,
+                                 long long b_cs, uint64_t *out, long long out_cs,
+                                 const DevModulus *mods, ModMap mm, int N, int op) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y, cidx = blockIdx.z;
+    const DevModulus m = mods[mm(l)];
+    const long long o = (long long)l * N + i;
+    const uint64_t x = a[cidx * a_cs + o], y = b[cidx * b_cs + o];
+    uint64_t r;
+    if (op == kEwAdd)
+        r = add_mod(x, y, m.q);
+    else if (op == kEwSub)
+        r = sub_mod(x, y, m.q);
+    else
+        r = mulmod_dev(x, y, m);
+    out[cidx * out_cs + o] = r;
+}
+
+void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const uint64_t *b,
+                      long long b_cs, uint64_t *out, long long out_cs, int ncomp, int nl, ModMap mm,
+                      int op, cudaStream_t st) {
+    if (ncomp <= 0 || nl <= 0) return;
+    ProfScope ps(c, PK_ELEMENTWISE, st, 8.0 * c.N * nl * (2.0 * ncomp + (b_cs ? ncomp : 1)));
+    note_launch();
+    ew_binary_kernel<<<grid_for(c.N, nl, ncomp), kBlock, 0, st>>>(a, a_cs, b, b_cs, out, out_cs,
+                                                                  c.d_mods, mm, c.N, op);
+}
+
 // ----------------------------------------------------------------------------
 // rescale (DivRoundByLastModulus)
 // ----------------------------------------------------------------------------

@@ -114,6 +114,12 @@ void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b,
 void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
                       const uint64_t *mform_const, uint64_t *out, long long out_pstride, int nl,
                       ModMap mm, int npolys, cudaStream_t st);
+// out_c = a_c op b_c (mod q) for ncomp components of nl limbs; b_cs = 0
+// applies one b polynomial to every component.  op: kEwAdd, kEwSub, kEwMul.
+enum : int { kEwAdd = 0, kEwSub = 1, kEwMul = 2 };
+void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const uint64_t *b,
+                      long long b_cs, uint64_t *out, long long out_cs, int ncomp, int nl, ModMap mm,
+                      int op, cudaStream_t st);
 // acc += x
 void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModMap mm,
                 cudaStream_t st);
