@@ -378,3 +378,56 @@ class CKKSEncoder:
 def precision_bits(got: np.ndarray, want: np.ndarray) -> float:
     err = np.max(np.abs(got - want))
     return float(-np.log2(err)) if err > 0 else 64.0
+
+
+# ----------------------------------------------------------------------------
+# Galois keys (rotations / conjugation)
+# ----------------------------------------------------------------------------
+
+
+def automorphism_int(s: np.ndarray, galois: int) -> np.ndarray:
+    """X -> X^galois on a signed coefficient vector (Lattigo ring.Permute)."""
+    n = len(s)
+    out = np.zeros(n, dtype=np.int64)
+    for i in range(n):
+        raw = i * galois
+        v = int(s[i])
+        out[raw % n] = -v if (raw // n) % 2 else v
+    return out
+
+
+def mkf_rotation_keys(R: RNS, keys: MKFKeys, galois: int, seed: int) -> np.ndarray:
+    """One sigma(s_i) -> s_E switching key per party (the paper evaluator's
+    rotation keys, software/mkf/mkf_cpu/true_mkf_ckks.go:321-360)."""
+    agg_ntt = R.qp_secret_ntt(keys.aggregate)
+    out = []
+    for i, s in enumerate(keys.secrets):
+        ss = R.qp_secret_ntt(automorphism_int(s, galois))
+        out.append(mkf_switching_key(R, ss, agg_ntt, rng(seed * 1000 + 300 + i)))
+    return np.stack(out)
+
+
+def kklss_galois_keys(R: RNS, keys: KKLSSKeys, galois: int, seed: int, conjugation: bool = False):
+    """KKLSS GenRotationKey / GenConjugationKey (software/kklss/mkrlwe/
+    keygen.go:190-268) for every party, with a fresh CRS vector (CRS[rot] or
+    CRS[-2]).  Rotation: rk = e + P s g - a sigma^-1(s); conjugation:
+    ck = e + P sigma(s) g - a s.  Returns (keys [k][beta][nQ+nP][N] MForm,
+    CRS stored [beta][nQ+nP][N])."""
+    alpha = R.np_ // 2
+    beta = (R.nq + alpha - 1) // alpha
+    g0 = rng(seed * 7919 + 17)
+    a_true, crs = _crs(R, beta, g0)
+    n2 = 2 * R.n
+    out = []
+    for i, s in enumerate(keys.secrets):
+        g = rng(seed * 7919 + 400 + i)
+        s_ntt = R.qp_secret_ntt(s)
+        if conjugation:
+            gad = kklss_switch_part(R, R.qp_secret_ntt(automorphism_int(s, galois)), g, gamma=2)
+            sub = s_ntt
+        else:
+            gad = kklss_switch_part(R, s_ntt, g, gamma=2)
+            sub = R.qp_secret_ntt(automorphism_int(s, pow(galois, -1, n2)))
+        k_ = [R.qp_sub(gad[j], R.qp_mul(a_true[j], sub)) for j in range(beta)]
+        out.append(np.stack([R.qp_pack(R.qp_mform(x)) for x in k_]))
+    return np.stack(out), crs

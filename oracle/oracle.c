@@ -1076,6 +1076,34 @@ static void ext_hoisted(const octx *c, int level, int beta, const uint64_t *a,
     free(acc);
 }
 
+void oracle_kklss_external_product(const octx *c, int level, const uint64_t *a_coeff,
+                                   const uint64_t *bg, uint64_t *out) {
+    int alpha = c->nP / 2;
+    int beta = (level + 1 + alpha - 1) / alpha;
+    uint64_t *dig = alloc_limbs(c, beta * (level + 1 + c->nP));
+    decompose_q(c, 2, level, a_coeff, dig);
+    ext_hoisted(c, level, beta, dig, bg, out);
+    free(dig);
+}
+
+void oracle_automorphism(const octx *c, int level, const uint64_t *in, uint64_t galois,
+                         uint64_t *out) {
+    int N = c->N;
+    uint64_t mask = (uint64_t)N - 1;
+    int logN = 0;
+    while ((1 << logN) < N) logN++;
+    for (int j = 0; j <= level; j++) {
+        uint64_t q = c->rQ.q[j];
+        const uint64_t *a = in + (size_t)j * N;
+        uint64_t *b = out + (size_t)j * N;
+        for (uint64_t i = 0; i < (uint64_t)N; i++) {
+            uint64_t raw = i * galois;
+            uint64_t x = a[i] % q;
+            b[raw & mask] = ((raw >> logN) & 1) ? (x ? q - x : 0) : x;
+        }
+    }
+}
+
 /* x/y gadget accumulation: acc[i] += key[i] (.) digits[i] for every digit;
  * finally MFormLvl (keyswitch_hoisted.go:84-123).  acc: [beta][L1+nP][N]. */
 static void gadget_accumulate(const octx *c, int level, int beta,

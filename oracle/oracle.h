@@ -132,6 +132,20 @@ int oracle_kklss_bfv_mulrelin(const octx *c, int k, const uint8_t *has0,
                               const uint64_t *crs_u, uint64_t t,
                               uint64_t *out);
 
+/* Galois automorphism X -> X^g on the coefficient domain of Q limbs
+ * [0, level] (the permutation loop of software/kklss/mkrlwe/keyswitch.go:
+ * 276-296 and Lattigo ring.Permute): out[i*g mod N] = +-in[i], negated when
+ * floor(i*g / N) is odd.  Canonical output. */
+void oracle_automorphism(const octx *c, int level, const uint64_t *in, uint64_t galois,
+                         uint64_t *out);
+
+/* KKLSS external product with a gadget vector (ExternalProductHoisted of
+ * the gamma = 2 decomposition, keyswitch_hoisted.go:11-45 after
+ * keyswitch.go:50-76): a coefficient domain at `level`, bg
+ * [betaMax][nQ+nP][N] (MForm, NTT); out coefficient domain. */
+void oracle_kklss_external_product(const octx *c, int level, const uint64_t *a_coeff,
+                                   const uint64_t *bg, uint64_t *out);
+
 /* Lattigo ModExp and prime helpers exposed for the test-side key
  * generator. */
 uint64_t oracle_mform(uint64_t a, uint64_t q);

@@ -66,6 +66,8 @@ def lib():
     L.oracle_kklss_bfv_mulrelin.restype = i
     L.oracle_kklss_bfv_mulrelin.argtypes = [vp, i, _u8p, _u8p, _u64p, _u64p, _u64p,
                                             _u64p, ctypes.c_uint64, _u64p]
+    L.oracle_automorphism.argtypes = [vp, i, _u64p, ctypes.c_uint64, _u64p]
+    L.oracle_kklss_external_product.argtypes = [vp, i, _u64p, _u64p, _u64p]
     L.oracle_mform.restype = ctypes.c_uint64
     L.oracle_mform.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
     for name in ("oracle_poly_mul", "oracle_poly_add", "oracle_poly_sub"):
@@ -278,6 +280,74 @@ class Oracle:
             ctypes.byref(so), _p(out))
         flat = out.reshape(-1)[: (k + 1) * (lv + 1) * self.n]
         return np.ascontiguousarray(flat.reshape(k + 1, lv + 1, self.n)), lv, so.value
+
+    # Galois automorphisms and rotations -----------------------------------
+    def galois_element(self, rotation: int) -> int:
+        """Lattigo GaloisElementForColumnRotationBy: 5^r mod 2N, r taken mod N/2."""
+        return pow(5, rotation % (self.n // 2), 2 * self.n)
+
+    def conjugation_element(self) -> int:
+        """GaloisElementForRowRotation: 2N - 1."""
+        return 2 * self.n - 1
+
+    def automorphism(self, level, a, galois):
+        """X -> X^galois on the coefficient domain of Q limbs [0, level]."""
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        out = np.empty_like(a)
+        for c in range(a.size // ((level + 1) * self.n)):
+            x = np.ascontiguousarray(a.reshape(-1, level + 1, self.n)[c])
+            y = np.empty_like(x)
+            self.L.oracle_automorphism(self.ctx, level, _p(x), int(galois), _p(y))
+            out.reshape(-1, level + 1, self.n)[c] = y
+        return out
+
+    def automorphism_ntt(self, level, a, galois):
+        """mkfAutomorphismNTT (true_mkf_ckks.go:307-320): InvNTT, permute, NTT."""
+        return self.ntt(self.automorphism(level, self.intt(a, "Q"), galois), "Q")
+
+    def kklss_external_product(self, level, a_coeff, bg):
+        a = np.ascontiguousarray(a_coeff, dtype=np.uint64)
+        out = np.zeros((level + 1, self.n), np.uint64)
+        self.L.oracle_kklss_external_product(self.ctx, level, _p(a), _p(np.ascontiguousarray(bg)), _p(out))
+        return out
+
+    def kklss_rotate(self, level, ct, rot_keys, crs, galois):
+        """KKLSS rotation (RotateHoisted, software/kklss/mkrlwe/keyswitch_hoisted.go:
+        198-249): c0 += sum_i Ext(c_i, rk_i); c_i = Ext(c_i, CRS[rot]); then
+        every component permuted.  ct: [k+1][level+1][N] coefficient domain."""
+        k = ct.shape[0] - 1
+        out = np.empty_like(ct)
+        c0 = ct[0].copy()
+        for i in range(k):
+            c0 = self.add(c0, self.kklss_external_product(level, ct[i + 1], rot_keys[i]))
+            out[i + 1] = self.kklss_external_product(level, ct[i + 1], crs)
+        out[0] = c0
+        return self.automorphism(level, out, galois)
+
+    def kklss_conjugate(self, level, ct, conj_keys, crs, galois):
+        """KKLSS conjugation (Conjugate, keyswitch.go:301-343, with the gadget
+        product of keyswitch_hoisted.go:11-45): every component permuted, then
+        c0 += sum_i Ext(c_i, ck_i); c_i = Ext(c_i, CRS[-2])."""
+        k = ct.shape[0] - 1
+        p = self.automorphism(level, ct, galois)
+        out = p.copy()
+        for i in range(k):
+            out[0] = self.add(out[0], self.kklss_external_product(level, p[i + 1], conj_keys[i]))
+            out[i + 1] = self.kklss_external_product(level, p[i + 1], crs)
+        return out
+
+    def mkf_rotate(self, level, ct, rot_keys, galois):
+        """MKF paper RotateNew (true_mkf_ckks.go:323-353): sigma(C0) + sum_i
+        switchOne(sigma(c_i), rk_i)[0], and sum_i switchOne(...)[1]; NTT domain.
+        Returns the compact pair."""
+        k = ct.shape[0] - 1
+        a0 = self.automorphism_ntt(level, ct[0], galois)
+        a1 = np.zeros_like(a0)
+        for i in range(k):
+            u0, u1 = self.mkf_switch_one(level, self.automorphism_ntt(level, ct[i + 1], galois),
+                                         rot_keys[i], True, True)
+            a0, a1 = self.add(a0, u0), self.add(a1, u1)
+        return np.stack([a0, a1])
 
     def kklss_bfv_mulrelin(self, k, has0, has1, op0, op1, rlk, crs_u, t):
         h0 = np.ascontiguousarray(np.array(has0, np.uint8))
