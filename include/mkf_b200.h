@@ -133,7 +133,9 @@ mkf_status mkf_ct_download_async(const mkf_ct *ct, uint64_t *host, size_t n_word
 /* MKF aggregate-fold construction                                      */
 /* ------------------------------------------------------------------ */
 /* The online key bundle of one party subset: k fold keys s_i -> s_E and
- * the relinearization key s_E^2 -> s_E (mkf_cpu/common.go:27-51). */
+ * the relinearization key s_E^2 -> s_E (mkf_cpu/common.go:27-51).  relin may
+ * be NULL for a bundle used only to fold or rotate (the k slots then hold
+ * the keys of those operations); products with it give MKF_ERR_MISSING_KEY. */
 mkf_status mkf_mkf_keyset_create(mkf_ctx *ctx, const mkf_key *const *fold, int k,
                                  const mkf_key *relin, mkf_mkf_keyset **out);
 void mkf_mkf_keyset_destroy(mkf_mkf_keyset *ks);
@@ -197,6 +199,41 @@ mkf_status mkf_kklss_union(const mkf_ct *op0, const mkf_ct *op1, int32_t *ids, i
  * and scale are set.  Missing keys give MKF_ERR_MISSING_KEY. */
 mkf_status mkf_kklss_mulrelin(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
                               const mkf_kklss_keyset *ks, mkf_ct *out, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* rotations and conjugation (Galois key switches)                      */
+/* ------------------------------------------------------------------ */
+/* Galois element of a slot rotation by `rotation` (Lattigo
+ * GaloisElementForColumnRotationBy: 5^r mod 2N, r taken mod N/2) and of the
+ * conjugation (GaloisElementForRowRotation: 2N - 1). */
+uint64_t mkf_galois_element(const mkf_ctx *ctx, int rotation);
+uint64_t mkf_conjugation_element(const mkf_ctx *ctx);
+/* KKLSS Galois keys of one element: the CRS vector it was made with (CRS[rot]
+ * for a rotation, CRS[-2] for the conjugation; MKF_KEY_GADGET) and one
+ * MKF_KEY_GADGET key per party (mkrlwe/keygen.go:190-268, RotationKeySet /
+ * ConjugationKeySet, mkrlwe/keys.go:125-220). */
+typedef struct mkf_galois_keyset mkf_galois_keyset;
+mkf_status mkf_galois_keyset_create(mkf_ctx *ctx, uint64_t galois, const mkf_key *crs,
+                                    int conjugation, mkf_galois_keyset **out);
+mkf_status mkf_galois_keyset_add(mkf_galois_keyset *ks, int32_t party_id, const mkf_key *key);
+void mkf_galois_keyset_destroy(mkf_galois_keyset *ks);
+/* KKLSS rotation / conjugation of a coefficient-domain ciphertext
+ * (mkckks.Evaluator.RotateHoistedNew / ConjugateNew, mkckks/evaluator.go:
+ * 533-621; RotateHoisted, mkrlwe/keyswitch_hoisted.go:198-249; Conjugate,
+ * keyswitch.go:301-343).  Each party component goes through the gadget
+ * product of the hoisted path (keyswitch_hoisted.go:11-45); the non-hoisted
+ * ExternalProduct of keyswitch.go:82-129 reuses one decomposition buffer for
+ * every digit and is not reproduced.  `out`: same components, level, ids and
+ * scale.  A missing party key gives MKF_ERR_MISSING_KEY. */
+mkf_status mkf_kklss_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_galois_keyset *ks,
+                            mkf_ct *out, void *stream);
+/* MKF paper rotation (paperMKFCKKSEvaluator.RotateNew, software/mkf/
+ * mkf_cpu/true_mkf_ckks.go:321-353): the (k+1)-component NTT-domain
+ * ciphertext mapped by `galois` and folded with one sigma(s_i) -> s_E key
+ * per party (the fold slots of `rot`; a key set made with relin = NULL).
+ * `out`: 2 components (compact) or k+1 (c0 then Gamma repeated). */
+mkf_status mkf_mkf_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *rot,
+                          uint64_t galois, mkf_ct *out, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* batched form                                                         */

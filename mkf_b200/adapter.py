@@ -16,24 +16,30 @@ linear layers, products) runs unchanged.
 * FoldToAggregate / MaterializeAggregate (foldCarrierToAggregate,
   materializeAggregate, :190-222).
 
-Rotations and polynomial evaluation (RotateNew, EvaluatePoly) need Galois
-keys and the polynomial evaluator, which this library does not provide;
-they raise NotImplementedError.  The collective refresh protocol is out of
-scope.
+* RotateNew / Rotate / RotateHoistedNew: the paper rotation with one
+  sigma(s_i) -> s_E key per party and Galois element (:130-160,
+  true_mkf_ckks.go:321-353), keys given per Galois element.
+
+Polynomial evaluation (EvaluatePoly) is not provided and raises
+NotImplementedError.  The collective refresh protocol is out of scope.
 """
 from __future__ import annotations
 
-from typing import Optional
+from typing import Dict, Optional
 
 from . import capi
-from .evaluator import Ciphertext, Evaluator, MKFEvaluator, MKFKeySet, Parameters
+from .evaluator import (Ciphertext, Evaluator, MKFEvaluator, MKFKeySet, Parameters,
+                        galois_element)
 
 
 class PaperMKFAdapter:
-    def __init__(self, params: Parameters, keys: MKFKeySet):
+    def __init__(self, params: Parameters, keys: MKFKeySet,
+                 rotations: Optional[Dict[int, MKFKeySet]] = None):
+        """rotations: Galois element -> key set of the k sigma(s_i) -> s_E keys."""
         if params.scheme != "ckks":
             raise ValueError("the paper interface is MK-CKKS")
         self.params, self.keys = params, keys
+        self.rotations = dict(rotations or {})
         self.parties = keys.k
         self._mkf = MKFEvaluator(params, keys)
         self._ev = Evaluator(params)
@@ -111,8 +117,24 @@ class PaperMKFAdapter:
         return out
 
     # not provided -----------------------------------------------------------
-    def RotateNew(self, ct, rotation):
-        raise NotImplementedError("rotations need Galois keys, which this library does not provide")
+    def RotateNew(self, ct: Ciphertext, rotation: int) -> Ciphertext:
+        self._check_carrier(ct, "Rotate")
+        if rotation % (self.params.N // 2) == 0:
+            out = self.NewCiphertext(ct.Level(), ct.Scale)
+            out.upload(ct.download())
+            return out
+        g = galois_element(self.params, rotation)
+        keys = self.rotations.get(g)
+        if keys is None or keys.k != self.parties:
+            raise capi.MissingKeyError(
+                5, f"party-specific Galois keys missing for rotation {rotation} (element {g})")
+        return self._mkf.RotateNew(ct, g, keys, materialize=True)
+
+    def Rotate(self, ct: Ciphertext, rotation: int, out: Ciphertext):
+        out.upload(self.RotateNew(ct, rotation).download())
+
+    def RotateHoistedNew(self, ct: Ciphertext, rotations):
+        return {r: self.RotateNew(ct, r) for r in rotations}
 
     def EvaluatePoly(self, ct, polynomial, targetScale):
         raise NotImplementedError("polynomial evaluation is not provided by this library")

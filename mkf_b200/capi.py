@@ -144,6 +144,13 @@ def lib():
         "mkf_add": (i, [vp, vp, vp, vp, vp]),
         "mkf_sub": (i, [vp, vp, vp, vp, vp]),
         "mkf_mul_plain": (i, [vp, vp, vp, vp, vp]),
+        "mkf_galois_element": (ctypes.c_uint64, [vp, i]),
+        "mkf_conjugation_element": (ctypes.c_uint64, [vp]),
+        "mkf_galois_keyset_create": (i, [vp, ctypes.c_uint64, vp, i, ctypes.POINTER(vp)]),
+        "mkf_galois_keyset_add": (i, [vp, ctypes.c_int32, vp]),
+        "mkf_galois_keyset_destroy": (None, [vp]),
+        "mkf_kklss_rotate": (i, [vp, vp, vp, vp, vp]),
+        "mkf_mkf_rotate": (i, [vp, vp, vp, ctypes.c_uint64, vp, vp]),
         "mkf_server_create": (i, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "mkf_job_scratch": (i, [ctypes.POINTER(Job), ctypes.POINTER(sz)]),
         "mkf_server_submit": (i, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]),

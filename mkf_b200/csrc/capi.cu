@@ -101,6 +101,7 @@ mkf_status prepare_mkf(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
     if (ks->ctx != ctx || left->ctx != ctx || right->ctx != ctx || out->ctx != ctx)
         return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
     const int k = ks->k;
+    if (!ks->relin) return fail(ctx, MKF_ERR_MISSING_KEY, "key set has no relinearization key");
     if (left->ncomp != k + 1 || right->ncomp != k + 1)
         return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
     const bool bfv = ctx->c.scheme == MKF_SCHEME_BFV;
@@ -498,9 +499,9 @@ mkf_status mkf_ct_download_async(const mkf_ct *ct, uint64_t *host, size_t n, voi
 
 mkf_status mkf_mkf_keyset_create(mkf_ctx *ctx, const mkf_key *const *fold, int k,
                                  const mkf_key *relin, mkf_mkf_keyset **out) {
-    if (!ctx || !out || !fold || !relin || k < 1 || k > kMaxParties) return MKF_ERR_INVALID_ARG;
+    if (!ctx || !out || !fold || k < 1 || k > kMaxParties) return MKF_ERR_INVALID_ARG;
     *out = nullptr;
-    if (relin->kind != MKF_KEY_SWITCHING || relin->ctx != ctx)
+    if (relin && (relin->kind != MKF_KEY_SWITCHING || relin->ctx != ctx))
         return fail(ctx, MKF_ERR_INVALID_ARG, "relinearization key must be a switching key");
     mkf_mkf_keyset *ks = new (std::nothrow) mkf_mkf_keyset();
     if (!ks) return MKF_ERR_OOM;
@@ -513,7 +514,7 @@ mkf_status mkf_mkf_keyset_create(mkf_ctx *ctx, const mkf_key *const *fold, int k
         }
         ks->fold.push_back(fold[i]->d);
     }
-    ks->relin = relin->d;
+    ks->relin = relin ? relin->d : nullptr;
     *out = ks;
     return MKF_OK;
 }
@@ -625,6 +626,109 @@ mkf_status mkf_sub(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, 
 mkf_status mkf_mul_plain(mkf_ctx *ctx, const mkf_ct *ct, const mkf_ct *pt, mkf_ct *out,
                          void *stream) {
     return ew_entry(ctx, ct, pt, out, kEwMul, stream);
+}
+
+uint64_t mkf_galois_element(const mkf_ctx *ctx, int rotation) {
+    if (!ctx) return 0;
+    const long long half = ctx->c.N / 2, m = 2LL * ctx->c.N;
+    long long r = rotation % half;
+    if (r < 0) r += half;
+    uint64_t g = 1, b = 5;
+    for (long long e = r; e; e >>= 1, b = (b * b) % (uint64_t)m)
+        if (e & 1) g = (g * b) % (uint64_t)m;
+    return g;
+}
+
+uint64_t mkf_conjugation_element(const mkf_ctx *ctx) { return ctx ? 2ull * ctx->c.N - 1 : 0; }
+
+mkf_status mkf_galois_keyset_create(mkf_ctx *ctx, uint64_t galois, const mkf_key *crs,
+                                    int conjugation, mkf_galois_keyset **out) {
+    if (!ctx || !crs || !out) return MKF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!(galois & 1) || galois >= 2ull * ctx->c.N)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "Galois element must be odd and below 2N");
+    if (crs->kind != MKF_KEY_GADGET || crs->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "the CRS vector must be a gadget vector");
+    mkf_galois_keyset *ks = new (std::nothrow) mkf_galois_keyset();
+    if (!ks) return MKF_ERR_OOM;
+    ks->ctx = ctx;
+    ks->galois = galois;
+    ks->conjugation = conjugation != 0;
+    ks->crs = crs->d;
+    *out = ks;
+    return MKF_OK;
+}
+
+mkf_status mkf_galois_keyset_add(mkf_galois_keyset *ks, int32_t party_id, const mkf_key *key) {
+    if (!ks || !key) return MKF_ERR_INVALID_ARG;
+    if (key->kind != MKF_KEY_GADGET || key->ctx != ks->ctx)
+        return fail(ks->ctx, MKF_ERR_INVALID_ARG, "a Galois key is a gadget vector of this context");
+    ks->keys[party_id] = key;
+    return MKF_OK;
+}
+
+void mkf_galois_keyset_destroy(mkf_galois_keyset *ks) { delete ks; }
+
+mkf_status mkf_kklss_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_galois_keyset *ks,
+                            mkf_ct *out, void *stream) {
+    if (!ctx || !in || !ks || !out) return MKF_ERR_INVALID_ARG;
+    if (in->ctx != ctx || ks->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    if (in->is_ntt) return fail(ctx, MKF_ERR_INVALID_ARG, "KKLSS operands must be in the coefficient domain");
+    if (out->ncomp != in->ncomp || out->level != in->level)
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have " + std::to_string(in->ncomp) + " components at level " +
+                        std::to_string(in->level));
+    const int k = in->ncomp - 1;
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) {
+        auto it = ks->keys.find(in->ids[i]);
+        if (it == ks->keys.end())
+            return fail(ctx, MKF_ERR_MISSING_KEY,
+                        "there is no Galois key with id " + std::to_string(in->ids[i]));
+        kp.p[i] = it->second->d;
+    }
+    const Operand I{in->d, in->cs(), in->ncomp, in->level};
+    cudaStream_t st = pick(ctx, stream);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return kklss_galois(ctx->c, a, st, k, in->level, I, kp, ks->crs, ks->galois,
+                            ks->conjugation != 0, out->d, out->cs());
+    });
+    if (s == MKF_OK) {
+        out->ids = in->ids;
+        out->scale = in->scale;
+        out->is_ntt = 0;
+    }
+    return s;
+}
+
+mkf_status mkf_mkf_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *rot,
+                          uint64_t galois, mkf_ct *out, void *stream) {
+    if (!ctx || !in || !rot || !out) return MKF_ERR_INVALID_ARG;
+    if (in->ctx != ctx || rot->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    if (ctx->c.scheme != MKF_SCHEME_CKKS || !in->is_ntt)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "MKF rotation takes NTT-domain MK-CKKS ciphertexts");
+    const int k = rot->k;
+    if (in->ncomp != k + 1) return fail(ctx, MKF_ERR_INVALID_ARG, "component/key count mismatch");
+    if (out->level != in->level || (out->ncomp != 2 && out->ncomp != k + 1))
+        return fail(ctx, MKF_ERR_INVALID_ARG,
+                    "output must have 2 or " + std::to_string(k + 1) + " components at level " +
+                        std::to_string(in->level));
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) kp.p[i] = rot->fold[i];
+    const Operand I{in->d, in->cs(), in->ncomp, in->level};
+    cudaStream_t st = pick(ctx, stream);
+    mkf_status s = run(ctx, st, [&](Arena &a) {
+        return mkf_rotate(ctx->c, a, st, k, in->level, I, kp, galois, out->ncomp, out->d, out->cs());
+    });
+    if (s == MKF_OK) {
+        out->scale = in->scale;
+        out->is_ntt = 1;
+    }
+    return s;
 }
 
 mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out) {

@@ -216,6 +216,97 @@ std::string mkf_fold(const Context &c, Arena &ar, cudaStream_t st, int scheme, i
     return "";
 }
 
+std::string mkf_rotate(const Context &c, Arena &ar, cudaStream_t st, int k, int level,
+                       const Operand &in, const KeyPtrs &rot, uint64_t galois, int n_out,
+                       uint64_t *out, long long out_cs) {
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (level < 0 || level >= c.nQ) return "level out of range";
+    if (c.nP > 8) return "at most 8 special primes are supported";
+    if (in.ncomp < k + 1) return "operand has fewer than k+1 components";
+    if (!(galois & 1) || galois >= 2ull * c.N) return "Galois element must be odd and below 2N";
+    if (n_out < 2) return "output needs at least two components";
+    const long long poly = (long long)(level + 1) * c.N;
+    uint64_t *perm = ar.take((k + 1) * poly);
+    FoldScratch f = take_fold_scratch(c, ar, false, k, level, 1);
+    uint64_t *F = ar.take(2 * poly);
+    if (ar.dry) return "";
+    launch_automorphism(c, in.data, in.cs, perm, poly, k + 1, level + 1, galois, true, st);
+    const Operand P{perm, poly, k + 1, level};
+    fold_sides(c, st, false, k, level, &P, 1, rot, f, F);
+    d2d2(out, out_cs, F, poly, poly, 1, st);
+    launch_replicate(F + poly, out + out_cs, poly, n_out - 1, out_cs, st);
+    return "";
+}
+
+std::string kklss_galois(const Context &c, Arena &ar, cudaStream_t st, int k, int level,
+                         const Operand &in, const KeyPtrs &keys, const uint64_t *crs,
+                         uint64_t galois, bool conjugation, uint64_t *out, long long out_cs) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1;
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (nP % 2) return "KKLSS needs an even number of special primes";
+    if (nP / 2 > 8) return "at most 16 special primes are supported";
+    if (level < 0 || level >= nQ) return "level out of range";
+    if (in.ncomp < k + 1) return "operand has fewer than k+1 components";
+    if (!(galois & 1) || galois >= 2ull * N) return "Galois element must be odd and below 2N";
+    const int beta = c.beta_of(level, 2);
+    const long long poly = (long long)L1 * N, qp = (long long)(L1 + nP) * N;
+    const long long kq = (long long)(nQ + nP) * N, kk = k;
+    uint64_t *perm = conjugation ? ar.take((k + 1) * poly) : nullptr;
+    uint64_t *res = conjugation ? nullptr : ar.take((k + 1) * poly);
+    uint64_t *H = ar.take(kk * beta * qp);
+    uint64_t *E = ar.take(2 * kk * qp);
+    uint64_t *tmp = ar.take(2 * kk * poly);
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, beta, k));
+    if (ar.dry) return "";
+    const uint64_t *src = in.data;
+    long long scs = in.cs;
+    if (conjugation) {
+        launch_automorphism(c, in.data, in.cs, perm, poly, k + 1, L1, galois, false, st);
+        src = perm;
+        scs = poly;
+    }
+    // hoisted gamma = 2 digits of every party component
+    decompose_ntt(c, src + scs, scs, 0, level, 2, beta, H, k, dscr, st);
+    // E[i] = digits_i . key_i, E[k + i] = digits_i . crs
+    IpArgs ip;
+    ip.A = H;
+    ip.a_gstride = beta * qp;
+    ip.a_tstride = qp;
+    ip.use_bptr = 1;
+    for (int i = 0; i < k; ++i) ip.bptr[i] = keys.p[i];
+    ip.b_tstride = kq;
+    ip.b_qlimbs = nQ;
+    ip.out = E;
+    ip.out_gstride = qp;
+    ip.nterms = beta;
+    ip.groups = k;
+    ip.L1 = L1;
+    ip.nP = nP;
+    launch_ip(c, ip, st);
+    IpArgs ia = ip;
+    ia.use_bptr = 0;
+    ia.B = crs;
+    ia.b_gstride = 0;
+    ia.out = E + kk * qp;
+    launch_ip(c, ia, st);
+    // ModDown of all 2k products, coefficient domain
+    moddown_prepare(c, st, E, qp, 2 * k, L1, 0, tmp);
+    uint64_t *dst = conjugation ? out : res;
+    const long long dcs = conjugation ? out_cs : poly;
+    d2d2(dst, dcs, src, scs, poly, 1, st);
+    {
+        CombineSpec s = pdown(c, E, qp, tmp, poly, dst, dcs, 1);
+        s.x_tstride = qp;
+        s.y_tstride = poly;
+        s.terms = k;
+        launch_moddown_combine(c, s, L1, qmap(L1), 1, st);
+    }
+    launch_moddown_combine(c, pdown(c, E + kk * qp, qp, tmp + kk * poly, poly, dst + dcs, dcs, 0),
+                           L1, qmap(L1), k, st);
+    if (!conjugation) launch_automorphism(c, res, poly, out, out_cs, k + 1, L1, galois, false, st);
+    return "";
+}
+
 std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
                          int level, const Operand &left, const Operand &right,
                          const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,

@@ -75,6 +75,23 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
 std::string mkf_fold(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k, int level,
                      const Operand &in, const KeyPtrs &fold, uint64_t *out, long long out_cs);
 
+// MKF paper rotation (RotateNew, software/mkf/mkf_cpu/true_mkf_ckks.go:
+// 323-353): every component mapped by X -> X^galois in the NTT domain, then
+// folded with the per-party sigma(s_i) -> s_E keys; out: c0 then the second
+// fold output n_out - 1 times (n_out = 2: compact).  CKKS (NTT domain).
+std::string mkf_rotate(const Context &c, Arena &ar, cudaStream_t st, int k, int level,
+                       const Operand &in, const KeyPtrs &rot, uint64_t galois, int n_out,
+                       uint64_t *out, long long out_cs);
+
+// KKLSS rotation (RotateHoisted, software/kklss/mkrlwe/keyswitch_hoisted.go:
+// 198-249) or, with conjugation, Conjugate (keyswitch.go:301-343): c0 +=
+// sum_i Ext(c_i, key_i), c_i = Ext(c_i, crs), with the permutation after
+// (rotation) or before (conjugation) the key switch.  Coefficient domain;
+// keys.p[i] and crs are [betaMax][nQ+nP][N] gadget vectors (MForm, NTT).
+std::string kklss_galois(const Context &c, Arena &ar, cudaStream_t st, int k, int level,
+                         const Operand &in, const KeyPtrs &keys, const uint64_t *crs,
+                         uint64_t galois, bool conjugation, uint64_t *out, long long out_cs);
+
 // KKLSS mult+relin with per-party (b, d, v) keys (software/kklss/mkckks/
 // evaluator.go:419-446,561-586; software/kklss/mkbfv/evaluator.go:85-152).
 // op0/op1: component 0 then one component per party of the union party set

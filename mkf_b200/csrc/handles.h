@@ -48,6 +48,14 @@ struct mkf_mkf_keyset {
     const uint64_t *relin = nullptr;
 };
 
+struct mkf_galois_keyset {
+    mkf_ctx *ctx = nullptr;
+    uint64_t galois = 0;
+    int conjugation = 0;
+    const uint64_t *crs = nullptr;
+    std::map<int32_t, const mkf_key *> keys;
+};
+
 struct mkf_kklss_keyset {
     mkf_ctx *ctx = nullptr;
     const uint64_t *crs_u = nullptr;

@@ -534,6 +534,51 @@ void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const
 }
 
 // ----------------------------------------------------------------------------
+// Galois automorphisms X -> X^g
+// ----------------------------------------------------------------------------
+// Coefficient domain (software/kklss/mkrlwe/keyswitch.go:276-296, Lattigo
+// ring.Permute): out[i*g mod N] = in[i], negated when floor(i*g/N) is odd.
+__global__ void automorphism_coeff_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
+                                          long long out_cs, const DevModulus *mods, int N, int logN,
+                                          uint64_t g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = blockIdx.y, cidx = blockIdx.z;
+    const uint64_t q = mods[l].q;
+    const uint64_t raw = (uint64_t)i * g;
+    const uint64_t x = in[cidx * in_cs + (long long)l * N + i];
+    const uint64_t v = ((raw >> logN) & 1) ? (x ? q - x : 0) : x;
+    out[cidx * out_cs + (long long)l * N + (long long)(raw & (uint64_t)(N - 1))] = v;
+}
+
+// NTT domain: slot j holds a(psi^(2 brev(j) + 1)), so sigma_g(a) at slot j is
+// a at the slot whose exponent is (2 brev(j) + 1) g mod 2N -- a gather.
+__global__ void automorphism_ntt_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
+                                        long long out_cs, int N, int logN, uint64_t g) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const int l = blockIdx.y, cidx = blockIdx.z;
+    const uint64_t e = 2ull * (__brev((unsigned)j) >> (32 - logN)) + 1;
+    const uint64_t e2 = (e * g) & (uint64_t)(2 * N - 1);
+    const int src = (int)(__brev((unsigned)((e2 - 1) >> 1)) >> (32 - logN));
+    out[cidx * out_cs + (long long)l * N + j] = in[cidx * in_cs + (long long)l * N + src];
+}
+
+void launch_automorphism(const Context &c, const uint64_t *in, long long in_cs, uint64_t *out,
+                         long long out_cs, int ncomp, int nl, uint64_t galois, bool ntt,
+                         cudaStream_t st) {
+    if (ncomp <= 0 || nl <= 0) return;
+    ProfScope ps(c, PK_ELEMENTWISE, st, 16.0 * c.N * nl * ncomp);
+    note_launch();
+    const dim3 grid = grid_for(c.N, nl, ncomp);
+    if (ntt)
+        automorphism_ntt_kernel<<<grid, kBlock, 0, st>>>(in, in_cs, out, out_cs, c.N, c.logN, galois);
+    else
+        automorphism_coeff_kernel<<<grid, kBlock, 0, st>>>(in, in_cs, out, out_cs, c.d_mods, c.N,
+                                                           c.logN, galois);
+}
+
+// ----------------------------------------------------------------------------
 // rescale (DivRoundByLastModulus)
 // ----------------------------------------------------------------------------
 __global__ void rescale_spread_kernel(const uint64_t *xL, long long xls, int L, uint64_t *t,

@@ -120,6 +120,11 @@ enum : int { kEwAdd = 0, kEwSub = 1, kEwMul = 2 };
 void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const uint64_t *b,
                       long long b_cs, uint64_t *out, long long out_cs, int ncomp, int nl, ModMap mm,
                       int op, cudaStream_t st);
+// Galois automorphism X -> X^galois (galois odd, < 2N) of ncomp components
+// of nl Q limbs, NTT or coefficient domain; out must not alias in.
+void launch_automorphism(const Context &c, const uint64_t *in, long long in_cs, uint64_t *out,
+                         long long out_cs, int ncomp, int nl, uint64_t galois, bool ntt,
+                         cudaStream_t st);
 // acc += x
 void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModMap mm,
                 cudaStream_t st);

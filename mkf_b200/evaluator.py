@@ -199,14 +199,17 @@ class RelinearizationKeySet:
 class MKFKeySet:
     """MKF online keys of one party subset: fold keys s_i -> s_E and relin."""
 
-    def __init__(self, params: Parameters, fold: Sequence[np.ndarray], relin: np.ndarray):
+    def __init__(self, params: Parameters, fold: Sequence[np.ndarray], relin: Optional[np.ndarray]):
+        """relin = None: a bundle of k keys used only to fold or rotate (for
+        instance one sigma(s_i) -> s_E key per party)."""
         self.params = params
         self.fold = [SwitchingKey(params, f) for f in fold]
-        self.relin = SwitchingKey(params, relin)
+        self.relin = SwitchingKey(params, relin) if relin is not None else None
         arr = (ctypes.c_void_p * len(self.fold))(*[f.handle for f in self.fold])
         h = ctypes.c_void_p()
-        capi.check(params.handle, capi.lib().mkf_mkf_keyset_create(params.handle, arr, len(self.fold),
-                                                                   self.relin.handle, ctypes.byref(h)))
+        capi.check(params.handle, capi.lib().mkf_mkf_keyset_create(
+            params.handle, arr, len(self.fold), self.relin.handle if self.relin else None,
+            ctypes.byref(h)))
         self.handle = h.value
         self.k = len(self.fold)
 
@@ -214,6 +217,42 @@ class MKFKeySet:
         try:
             if self.handle:
                 capi.lib().mkf_mkf_keyset_destroy(self.handle)
+        except Exception:
+            pass
+
+
+def galois_element(params: Parameters, rotation: int) -> int:
+    """5^r mod 2N (Lattigo GaloisElementForColumnRotationBy)."""
+    return int(capi.lib().mkf_galois_element(params.handle, int(rotation)))
+
+
+def conjugation_element(params: Parameters) -> int:
+    return int(capi.lib().mkf_conjugation_element(params.handle))
+
+
+class GaloisKeySet:
+    """KKLSS rotation or conjugation keys of one Galois element
+    (RotationKeySet / ConjugationKeySet): the CRS vector they were made with
+    and one gadget key per party."""
+
+    def __init__(self, params: Parameters, galois: int, crs: np.ndarray, conjugation: bool = False):
+        self.params, self.galois, self.conjugation = params, int(galois), conjugation
+        self.crs = Key(params, capi.KEY_GADGET, crs)
+        h = ctypes.c_void_p()
+        capi.check(params.handle, capi.lib().mkf_galois_keyset_create(
+            params.handle, self.galois, self.crs.handle, int(conjugation), ctypes.byref(h)))
+        self.handle = h.value
+        self.keys: Dict[int, Key] = {}
+
+    def AddKey(self, party_id: int, words: np.ndarray):
+        k = Key(self.params, capi.KEY_GADGET, words)
+        capi.check(self.params.handle, capi.lib().mkf_galois_keyset_add(self.handle, party_id, k.handle))
+        self.keys[party_id] = k
+
+    def __del__(self):
+        try:
+            if self.handle:
+                capi.lib().mkf_galois_keyset_destroy(self.handle)
         except Exception:
             pass
 
@@ -247,6 +286,31 @@ class Evaluator:
         out = Ciphertext(self.params, n.value + 1, level, False)
         capi.check(self.params.handle, L.mkf_kklss_mulrelin(self.params.handle, op0.handle, op1.handle,
                                                             rlkSet.handle, out.handle, stream))
+        return out
+
+    def Galois(self, ctIn: Ciphertext, keys: GaloisKeySet, ctOut: Ciphertext, stream=None):
+        capi.check(self.params.handle, capi.lib().mkf_kklss_rotate(
+            self.params.handle, ctIn.handle, keys.handle, ctOut.handle, stream))
+
+    def RotateNew(self, ctIn: Ciphertext, rotation: int, keys: GaloisKeySet) -> Ciphertext:
+        """mkckks.Evaluator.RotateHoistedNew (mkckks/evaluator.go:590-621):
+        slots rotated left by `rotation`."""
+        if rotation % (self.params.N // 2) == 0:
+            out = Ciphertext(self.params, ctIn.n_comp, ctIn.Level(), False, ctIn.ids, ctIn.Scale)
+            out.upload(ctIn.download())
+            return out
+        if keys.conjugation or keys.galois != galois_element(self.params, rotation):
+            raise capi.MissingKeyError(5, f"no rotation keys for rotation {rotation}")
+        out = Ciphertext(self.params, ctIn.n_comp, ctIn.Level(), False)
+        self.Galois(ctIn, keys, out)
+        return out
+
+    def ConjugateNew(self, ctIn: Ciphertext, keys: GaloisKeySet) -> Ciphertext:
+        """mkckks.Evaluator.ConjugateNew (mkckks/evaluator.go:533-544)."""
+        if not keys.conjugation:
+            raise capi.MissingKeyError(5, "no conjugation keys")
+        out = Ciphertext(self.params, ctIn.n_comp, ctIn.Level(), False)
+        self.Galois(ctIn, keys, out)
         return out
 
     def Rescale(self, ctIn: Ciphertext, minScale: float, ctOut: Ciphertext, stream=None):
@@ -283,6 +347,15 @@ class MKFEvaluator:
         n_out = self.keys.k + 1 if materialize else 2
         out = Ciphertext(self.params, n_out, lvl, self.params.scheme == "ckks")
         self.MulRelin(left, right, out, rescale, materialize, stream)
+        return out
+
+    def RotateNew(self, ct: Ciphertext, galois: int, rot_keys: "MKFKeySet",
+                  materialize: bool = True) -> Ciphertext:
+        """Paper RotateNew (true_mkf_ckks.go:321-353) with one
+        sigma(s_i) -> s_E key per party in rot_keys."""
+        out = Ciphertext(self.params, ct.n_comp if materialize else 2, ct.Level(), True)
+        capi.check(self.params.handle, capi.lib().mkf_mkf_rotate(
+            self.params.handle, ct.handle, rot_keys.handle, int(galois), out.handle, None))
         return out
 
     def MulRelin(self, left, right, out, rescale=True, materialize=False, stream=None):
