@@ -173,14 +173,30 @@ mkf_status mkf_mkf_materialize(mkf_ctx *ctx, const mkf_ct *compact, mkf_ct *out,
 /* ------------------------------------------------------------------ */
 /* The linear operations the paper adapter leaves to Lattigo's evaluator and
  * its public MulNew (true_mkf_ckks_adapter.go:80-127), applied to every
- * component: out = a + b or a - b (same component count, party ids, domain
- * and scale; level = the lower of the two), or out = ct * pt for a public
- * plaintext `pt` (one component, NTT domain like ct; scale multiplies).
+ * component: out = a + b or a - b (same component count, party ids and
+ * domain; level = the lower of the two; scales as Lattigo v2.3's Add: the
+ * smaller-scale operand is multiplied by uint64(larger/smaller) when that
+ * exceeds 1 and the result has the larger scale), or out = ct * pt for a
+ * public plaintext `pt` (one component, NTT domain like ct; scale
+ * multiplies).
  * `out` must have a's component count at the output level. */
 mkf_status mkf_add(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream);
 mkf_status mkf_sub(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_ct *out, void *stream);
 mkf_status mkf_mul_plain(mkf_ctx *ctx, const mkf_ct *ct, const mkf_ct *pt, mkf_ct *out,
                          void *stream);
+/* Copy of `in`'s components truncated to out's level (DropLevel when
+ * out->level < in->level); metadata copied. */
+mkf_status mkf_ct_copy(mkf_ctx *ctx, const mkf_ct *in, mkf_ct *out, void *stream);
+/* Constants on NTT-domain carriers, one residue per limb for each half of the
+ * slots (consts: host [out level + 1][2], canonical): Lattigo's AddConst
+ * (added to component 0) and MultByGaussianIntegerAndAdd / MultByConst
+ * (every component), as the paper polynomial evaluator calls them
+ * (true_mkf_ckks_polynomial.go:62-74, 219-273).  At most 64 limbs. */
+#define MKF_SLOT_MUL_ADD 0 /* out_u += in_u * c */
+#define MKF_SLOT_ADD_C0 1  /* out_0 = in_0 + c, out_u = in_u */
+#define MKF_SLOT_MUL 2     /* out_u = in_u * c */
+mkf_status mkf_slot_const(mkf_ctx *ctx, const mkf_ct *in, const uint64_t *consts, int mode,
+                          mkf_ct *out, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* KKLSS per-party-key construction                                     */

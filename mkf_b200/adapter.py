@@ -20,8 +20,10 @@ linear layers, products) runs unchanged.
   sigma(s_i) -> s_E key per party and Galois element (:130-160,
   true_mkf_ckks.go:321-353), keys given per Galois element.
 
-Polynomial evaluation (EvaluatePoly) is not provided and raises
-NotImplementedError.  The collective refresh protocol is out of scope.
+* EvaluatePoly: the reference's baby-step/giant-step schedule
+  (true_mkf_ckks_polynomial.go) over these operations (mkf_b200.polynomial).
+
+The collective refresh protocol is out of scope.
 """
 from __future__ import annotations
 
@@ -136,5 +138,10 @@ class PaperMKFAdapter:
     def RotateHoistedNew(self, ct: Ciphertext, rotations):
         return {r: self.RotateNew(ct, r) for r in rotations}
 
-    def EvaluatePoly(self, ct, polynomial, targetScale):
-        raise NotImplementedError("polynomial evaluation is not provided by this library")
+    def EvaluatePoly(self, ct: Ciphertext, polynomial, targetScale: float) -> Ciphertext:
+        """paperMKFCKKSEvaluator.EvaluatePoly (true_mkf_ckks_polynomial.go:79-111):
+        `polynomial` is a mkf_b200.polynomial.Polynomial in the standard or
+        Chebyshev basis (input already mapped for the latter)."""
+        from .polynomial import EvaluatePoly
+        self._check_carrier(ct, "EvaluatePoly")
+        return EvaluatePoly(self, ct, polynomial, targetScale)

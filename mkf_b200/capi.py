@@ -54,6 +54,7 @@ class ParamsDesc(ctypes.Structure):
     ]
 
 
+SLOT_MUL_ADD, SLOT_ADD_C0, SLOT_MUL = 0, 1, 2
 JOB_MKF, JOB_KKLSS = 1, 2
 BATCH_GRAPH = 1
 
@@ -151,6 +152,8 @@ def lib():
         "mkf_galois_keyset_destroy": (None, [vp]),
         "mkf_kklss_rotate": (i, [vp, vp, vp, vp, vp]),
         "mkf_mkf_rotate": (i, [vp, vp, vp, ctypes.c_uint64, vp, vp]),
+        "mkf_ct_copy": (i, [vp, vp, vp, vp]),
+        "mkf_slot_const": (i, [vp, vp, u64p, i, vp, vp]),
         "mkf_server_create": (i, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "mkf_job_scratch": (i, [ctypes.POINTER(Job), ctypes.POINTER(sz)]),
         "mkf_server_submit": (i, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]),

@@ -593,12 +593,29 @@ static mkf_status ew_entry(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_c
         if (b->ncomp != 1) return fail(ctx, MKF_ERR_INVALID_ARG, "the public operand must have 1 component");
         if (!a->is_ntt) return fail(ctx, MKF_ERR_INVALID_ARG, "public products need NTT-domain operands");
         scale = a->scale * b->scale;
-    } else {
+    }
+    // Lattigo v2.3 Add/Sub (evaluateInPlace): the operand with the smaller
+    // scale is first multiplied by uint64(larger / smaller) when that exceeds
+    // 1, and the result carries the larger scale
+    EwFactors fac;
+    if (op != kEwMul) {
         if (a->ncomp != b->ncomp || a->ids != b->ids)
             return fail(ctx, MKF_ERR_INVALID_ARG, "operands have different components or party ids");
-        const double d = a->scale - b->scale;
-        if (d > 1e-9 * a->scale || -d > 1e-9 * a->scale)
-            return fail(ctx, MKF_ERR_INVALID_ARG, "operands have different scales");
+        if (!(a->scale > 0) || !(b->scale > 0))
+            return fail(ctx, MKF_ERR_INVALID_ARG, "operands need positive scales");
+        uint64_t fa = 1, fb = 1;
+        if (a->scale > b->scale) fb = std::max<uint64_t>(1, (uint64_t)(a->scale / b->scale));
+        if (b->scale > a->scale) fa = std::max<uint64_t>(1, (uint64_t)(b->scale / a->scale));
+        scale = std::max(a->scale, b->scale);
+        if (fa > 1 || fb > 1) {
+            if (level + 1 > 64) return fail(ctx, MKF_ERR_UNSUPPORTED, "at most 64 limbs");
+            fac.on = 1;
+            for (int l = 0; l <= level; ++l) {
+                const uint64_t q = ctx->c.h_mods[l].q;
+                fac.fa[l] = fa % q;
+                fac.fb[l] = fb % q;
+            }
+        }
     }
     if (out->ncomp != a->ncomp || out->level != level)
         return fail(ctx, MKF_ERR_INVALID_ARG,
@@ -607,7 +624,7 @@ static mkf_status ew_entry(mkf_ctx *ctx, const mkf_ct *a, const mkf_ct *b, mkf_c
     cudaSetDevice(ctx->c.device);
     cudaStream_t st = pick(ctx, stream);
     launch_ew_binary(ctx->c, a->d, a->cs(), b->d, op == kEwMul ? 0 : b->cs(), out->d, out->cs(),
-                     a->ncomp, level + 1, qmap(level + 1), op, st);
+                     a->ncomp, level + 1, qmap(level + 1), op, st, fac.on ? &fac : nullptr);
     mkf_status s = cuda_check(ctx, "elementwise");
     if (s == MKF_OK) {
         out->scale = scale;
@@ -727,6 +744,56 @@ mkf_status mkf_mkf_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *
     if (s == MKF_OK) {
         out->scale = in->scale;
         out->is_ntt = 1;
+    }
+    return s;
+}
+
+mkf_status mkf_ct_copy(mkf_ctx *ctx, const mkf_ct *in, mkf_ct *out, void *stream) {
+    if (!ctx || !in || !out) return MKF_ERR_INVALID_ARG;
+    if (in->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    if (out->ncomp != in->ncomp || out->level > in->level)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "output must have the input's components at a level <= its level");
+    cudaSetDevice(ctx->c.device);
+    cudaStream_t st = pick(ctx, stream);
+    cudaMemcpy2DAsync(out->d, out->cs() * 8, in->d, in->cs() * 8, out->cs() * 8, in->ncomp,
+                      cudaMemcpyDeviceToDevice, st);
+    mkf_status s = cuda_check(ctx, "copy");
+    if (s == MKF_OK) {
+        out->scale = in->scale;
+        out->is_ntt = in->is_ntt;
+        out->ids = in->ids;
+    }
+    return s;
+}
+
+mkf_status mkf_slot_const(mkf_ctx *ctx, const mkf_ct *in, const uint64_t *consts, int mode,
+                          mkf_ct *out, void *stream) {
+    if (!ctx || !in || !consts || !out) return MKF_ERR_INVALID_ARG;
+    if (in->ctx != ctx || out->ctx != ctx)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "handles belong to another context");
+    if (mode < MKF_SLOT_MUL_ADD || mode > MKF_SLOT_MUL) return fail(ctx, MKF_ERR_INVALID_ARG, "unknown mode");
+    if (!in->is_ntt) return fail(ctx, MKF_ERR_INVALID_ARG, "slot constants need NTT-domain operands");
+    if (out->ncomp != in->ncomp || out->level > in->level)
+        return fail(ctx, MKF_ERR_INVALID_ARG, "output must have the input's components at a level <= its level");
+    const int nl = out->level + 1;
+    if (nl > kMaxSlotLimbs) return fail(ctx, MKF_ERR_UNSUPPORTED, "at most 64 limbs");
+    SlotConsts sc;
+    for (int l = 0; l < nl; ++l) {
+        const uint64_t q = ctx->c.h_mods[l].q;
+        if (consts[2 * l] >= q || consts[2 * l + 1] >= q)
+            return fail(ctx, MKF_ERR_INVALID_ARG, "constants must be canonical residues");
+        sc.c[l][0] = consts[2 * l];
+        sc.c[l][1] = consts[2 * l + 1];
+    }
+    cudaSetDevice(ctx->c.device);
+    cudaStream_t st = pick(ctx, stream);
+    launch_slot_const(ctx->c, in->d, in->cs(), out->d, out->cs(), in->ncomp, nl, sc, mode, st);
+    mkf_status s = cuda_check(ctx, "slot constants");
+    if (s == MKF_OK && mode != MKF_SLOT_MUL_ADD) {
+        out->scale = in->scale;
+        out->is_ntt = 1;
+        out->ids = in->ids;
     }
     return s;
 }

@@ -326,7 +326,20 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     const int nR = nQ + c.nQM;
     const long long rp = (long long)nR * N;
 
-    FoldScratch fs = take_fold_scratch(c, ar, bfv, k, level, 2);
+    // The reference folds each operand at its own level and multiplies the
+    // first level+1 limbs (true_mkf_ckks.go:253-272); a switch at a higher
+    // level is not the truncation of one at a lower level, so operands at
+    // different levels are folded separately.
+    const bool same = left.level == right.level;
+    FoldScratch fs = take_fold_scratch(c, ar, bfv, k, level, same ? 2 : 1);
+    FoldScratch fl, fr;
+    uint64_t *Fl = nullptr, *Fr = nullptr;
+    if (!same) {
+        fl = take_fold_scratch(c, ar, bfv, k, left.level, 1);
+        fr = take_fold_scratch(c, ar, bfv, k, right.level, 1);
+        Fl = ar.take(2LL * (left.level + 1) * N);
+        Fr = ar.take(2LL * (right.level + 1) * N);
+    }
     uint64_t *F = ar.take(4 * poly);
     uint64_t *mu = ar.take(3 * poly);
     uint64_t *rcoef = bfv ? nullptr : ar.take(poly);
@@ -344,8 +357,15 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     if (ar.dry) return "";
 
     // 1-3. fold both operands: F[s][0] = C0_s + sum_i p0, F[s][1] = sum_i p1
-    const Operand ops[2] = {left, right};
-    fold_sides(c, st, bfv, k, level, ops, 2, fold, fs, F);
+    if (same) {
+        const Operand ops[2] = {left, right};
+        fold_sides(c, st, bfv, k, level, ops, 2, fold, fs, F);
+    } else {
+        fold_sides(c, st, bfv, k, left.level, &left, 1, fold, fl, Fl);
+        fold_sides(c, st, bfv, k, right.level, &right, 1, fold, fr, Fr);
+        d2d2(F, poly, Fl, (long long)(left.level + 1) * N, poly, 2, st);
+        d2d2(F + 2 * poly, poly, Fr, (long long)(right.level + 1) * N, poly, 2, st);
+    }
 
     uint64_t *mu0 = mu, *mu1 = mu + poly, *mu2 = mu + 2 * poly;
     if (!bfv) {

@@ -503,16 +503,22 @@ void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModM
 }
 
 // out_c = a_c (op) b_c over ncomp components of nl limbs (b_cs = 0: one b
-// polynomial for every component, as a public plaintext is applied)
+// polynomial for every component, as a public plaintext is applied); for
+// add/sub, optional integer factors per limb scale a or b first.
 __global__ void ew_binary_kernel(const uint64_t *a, long long a_cs, const uint64_t *b,
                                  long long b_cs, uint64_t *out, long long out_cs,
-                                 const DevModulus *mods, ModMap mm, int N, int op) {
+                                 const DevModulus *mods, ModMap mm, int N, int op,
+                                 EwFactors f) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, cidx = blockIdx.z;
     const DevModulus m = mods[mm(l)];
     const long long o = (long long)l * N + i;
-    const uint64_t x = a[cidx * a_cs + o], y = b[cidx * b_cs + o];
+    uint64_t x = a[cidx * a_cs + o], y = b[cidx * b_cs + o];
+    if (f.on) {
+        x = mulmod_dev(x, f.fa[l], m);
+        y = mulmod_dev(y, f.fb[l], m);
+    }
     uint64_t r;
     if (op == kEwAdd)
         r = add_mod(x, y, m.q);
@@ -525,12 +531,50 @@ __global__ void ew_binary_kernel(const uint64_t *a, long long a_cs, const uint64
 
 void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const uint64_t *b,
                       long long b_cs, uint64_t *out, long long out_cs, int ncomp, int nl, ModMap mm,
-                      int op, cudaStream_t st) {
+                      int op, cudaStream_t st, const EwFactors *f) {
     if (ncomp <= 0 || nl <= 0) return;
     ProfScope ps(c, PK_ELEMENTWISE, st, 8.0 * c.N * nl * (2.0 * ncomp + (b_cs ? ncomp : 1)));
     note_launch();
+    EwFactors none;
     ew_binary_kernel<<<grid_for(c.N, nl, ncomp), kBlock, 0, st>>>(a, a_cs, b, b_cs, out, out_cs,
-                                                                  c.d_mods, mm, c.N, op);
+                                                                  c.d_mods, mm, c.N, op,
+                                                                  f ? *f : none);
+}
+
+// ----------------------------------------------------------------------------
+// per-limb constants on the two halves of the NTT slots
+// ----------------------------------------------------------------------------
+// In Lattigo's bit-reversed NTT order the first N/2 slots are the evaluation
+// points where X^(N/2) equals the fourth root of unity psi^(N/2) and the last
+// N/2 those where it equals its negative, so a Gaussian integer re + im*i (or
+// a complex constant) becomes one residue per half and limb.
+__global__ void slot_const_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
+                                  long long out_cs, SlotConsts sc, const DevModulus *mods, int N,
+                                  int mode) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const int l = blockIdx.y, u = blockIdx.z;
+    const DevModulus m = mods[l];
+    const uint64_t cst = sc.c[l][j >= (N >> 1)];
+    const long long o = (long long)l * N + j;
+    const uint64_t x = in[u * in_cs + o];
+    uint64_t &y = out[u * out_cs + o];
+    if (mode == kSlotMulAdd)
+        y = add_mod(y, mulmod_dev(x, cst, m), m.q);
+    else if (mode == kSlotMul)
+        y = mulmod_dev(x, cst, m);
+    else
+        y = u == 0 ? add_mod(x, cst, m.q) : x;
+}
+
+void launch_slot_const(const Context &c, const uint64_t *in, long long in_cs, uint64_t *out,
+                       long long out_cs, int ncomp, int nl, const SlotConsts &sc, int mode,
+                       cudaStream_t st) {
+    if (ncomp <= 0 || nl <= 0) return;
+    ProfScope ps(c, PK_ELEMENTWISE, st, 8.0 * c.N * nl * ncomp * (mode == kSlotMulAdd ? 3 : 2));
+    note_launch();
+    slot_const_kernel<<<grid_for(c.N, nl, ncomp), kBlock, 0, st>>>(in, in_cs, out, out_cs, sc,
+                                                                   c.d_mods, c.N, mode);
 }
 
 // ----------------------------------------------------------------------------

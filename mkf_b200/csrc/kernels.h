@@ -117,9 +117,26 @@ void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
 // out_c = a_c op b_c (mod q) for ncomp components of nl limbs; b_cs = 0
 // applies one b polynomial to every component.  op: kEwAdd, kEwSub, kEwMul.
 enum : int { kEwAdd = 0, kEwSub = 1, kEwMul = 2 };
+// Integer factors (residues per limb, at most 64 limbs) applied to a and b
+// before an add/sub; on = 0 leaves the operands as they are.
+struct EwFactors {
+    int on = 0;
+    uint64_t fa[64] = {}, fb[64] = {};
+};
 void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const uint64_t *b,
                       long long b_cs, uint64_t *out, long long out_cs, int ncomp, int nl, ModMap mm,
-                      int op, cudaStream_t st);
+                      int op, cudaStream_t st, const EwFactors *f = nullptr);
+// One residue per limb and half of the NTT slots (at most kMaxSlotLimbs limbs).
+constexpr int kMaxSlotLimbs = 64;
+struct SlotConsts {
+    uint64_t c[kMaxSlotLimbs][2];
+};
+enum : int { kSlotMulAdd = 0, kSlotAddC0 = 1, kSlotMul = 2 };
+// mode kSlotMulAdd: out_u += in_u * c; kSlotMul: out_u = in_u * c;
+// kSlotAddC0: out_0 = in_0 + c, out_u = in_u for u > 0.  NTT domain.
+void launch_slot_const(const Context &c, const uint64_t *in, long long in_cs, uint64_t *out,
+                       long long out_cs, int ncomp, int nl, const SlotConsts &sc, int mode,
+                       cudaStream_t st);
 // Galois automorphism X -> X^galois (galois odd, < 2N) of ncomp components
 // of nl Q limbs, NTT or coefficient domain; out must not alias in.
 void launch_automorphism(const Context &c, const uint64_t *in, long long in_cs, uint64_t *out,
