@@ -63,11 +63,7 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+from mkf_b200.replicas import Replicas, dist_env  # noqa: E402
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, ncu, one launch)
@@ -247,10 +243,7 @@ def run_gpu(a):
     import torch
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    reps = Replicas("nccl", timeout_s=300)
     from mkf_b200 import capi, params
     from mkf_b200 import evaluator as ev
 
@@ -285,20 +278,8 @@ def run_gpu(a):
         E.MulRelin(l, r, outs[i % nin], rescale=True, materialize=True,
                    stream=ctypes_stream(s))
 
-    def barrier():
-        torch.cuda.synchronize()
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = reps.barrier
+    max_over_ranks = reps.max_over_ranks
 
     # ---- plain: one product at a time on one stream -------------------------
     L = capi.lib()
@@ -470,9 +451,7 @@ def run_gpu(a):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    reps.close()
 
 
 import ctypes  # noqa: E402
