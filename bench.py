@@ -269,6 +269,9 @@ def run_gpu(a):
         l = ev.Ciphertext.from_array(P, random_limbs(g, lit.q[:L1], N, k + 1), True, scale=lit.scale)
         r = ev.Ciphertext.from_array(P, random_limbs(g, lit.q[:L1], N, k + 1), True, scale=lit.scale)
         ins.append((l, r))
+    # launch choices: time every candidate on this workload, keep the fastest
+    from mkf_b200 import autotune
+    tuned = autotune.tune_mkf(P, k, level, operands=(E, ins[0][0], ins[0][1]))
     lout = E.output_level(ins[0][0], ins[0][1], True)
     outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(nin)]
     streams = [torch.cuda.Stream() for _ in range(max(1, a.streams))]
@@ -444,6 +447,8 @@ def run_gpu(a):
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roofline,
+            "autotune": {"best": tuned["best"],
+                         "ms_per_product": tuned["ms"]},
             "batched_mix": mix,
             "serving": serve,
             "kernels": kinds,

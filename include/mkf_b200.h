@@ -252,6 +252,20 @@ mkf_status mkf_mkf_rotate(mkf_ctx *ctx, const mkf_ct *in, const mkf_mkf_keyset *
                           uint64_t galois, mkf_ct *out, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* launch tuning                                                        */
+/* ------------------------------------------------------------------ */
+/* Launch choices of a context (no counterpart in the reference; every
+ * choice computes the same words, only the time differs).  The autotuner
+ * (mkf_b200.autotune) times candidates and sets the fastest. */
+typedef struct mkf_tuning {
+    int fuse_ip;     /* 1: key-switch inner products fused into the digits' row pass */
+    int ip_block;    /* threads per block of the stand-alone inner product: 128, 256, 512 */
+    int modup_chunk; /* target limbs per thread of the party-summed ModUp: 8, 12, 24 */
+} mkf_tuning;
+mkf_status mkf_ctx_get_tuning(const mkf_ctx *ctx, mkf_tuning *out);
+mkf_status mkf_ctx_set_tuning(mkf_ctx *ctx, const mkf_tuning *t);
+
+/* ------------------------------------------------------------------ */
 /* batched form                                                         */
 /* ------------------------------------------------------------------ */
 /* No counterpart in the reference, which runs one product per call

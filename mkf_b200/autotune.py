@@ -1,0 +1,120 @@
+"""Launch autotuner: picks, per context and workload, the launch choices that
+make a product fastest on the device at hand.
+
+The choices (mkf_tuning) never change the words computed, only the time:
+whether the key-switch inner products run fused into the digits' row pass
+or as their own memory-bound kernel, the inner-product block size, and the
+number of target limbs a thread of the party-summed ModUp handles.  The
+tuner times a product per candidate with CUDA events (after a warm-up),
+keeps the fastest, sets it on the context, and can keep the result in a JSON
+cache keyed by device and workload shape.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import json
+import os
+from typing import Callable, Dict, Iterable, List, Optional, Tuple
+
+import numpy as np
+
+from . import capi
+
+AXES = {"fuse_ip": (0, 1), "ip_block": (128, 256, 512), "modup_chunk": (8, 12, 24)}
+
+
+def candidates(axes: Dict[str, Iterable] = AXES) -> List[dict]:
+    keys = list(axes)
+    return [dict(zip(keys, vals)) for vals in itertools.product(*(axes[k] for k in keys))]
+
+
+def get_tuning(params) -> dict:
+    t = capi.Tuning()
+    capi.check(params.handle, capi.lib().mkf_ctx_get_tuning(params.handle, ctypes.byref(t)))
+    return {f: getattr(t, f) for f, _ in capi.Tuning._fields_}
+
+
+def set_tuning(params, **kw):
+    cur = get_tuning(params)
+    cur.update(kw)
+    t = capi.Tuning(cur["fuse_ip"], cur["ip_block"], cur["modup_chunk"])
+    capi.check(params.handle, capi.lib().mkf_ctx_set_tuning(params.handle, ctypes.byref(t)))
+
+
+def search(cands: List[dict], time_fn: Callable[[dict], float]) -> Tuple[dict, Dict[str, float]]:
+    """Times every candidate once (time_fn sets it and returns ms) and
+    returns the fastest with the table of times."""
+    table, best, best_ms = {}, None, float("inf")
+    for cnd in cands:
+        ms = float(time_fn(cnd))
+        table[json.dumps(cnd, sort_keys=True)] = ms
+        if ms < best_ms:
+            best, best_ms = cnd, ms
+    return best, table
+
+
+def _cache_key(params, k: int, level: int) -> str:
+    import torch
+    lit = params.literal
+    name = torch.cuda.get_device_name(params.device) if torch.cuda.is_available() else "cpu"
+    return f"{name}|mkf-{params.scheme}|logN{lit.log_n}|Q{len(lit.q)}|P{len(lit.p)}|k{k}|L{level}"
+
+
+def tune_mkf(params, k: int, level: Optional[int] = None, reps: int = 3, keys=None, operands=None,
+             cache_path: Optional[str] = None, cands: Optional[List[dict]] = None) -> dict:
+    """Tunes the MKF mult+relin(+rescale) of k parties at `level` on this
+    context and leaves the fastest choice set.  keys/operands: an
+    (MKFEvaluator, left, right) triple to time on; random ones are made
+    otherwise.  Returns {"best": ..., "ms": {candidate: ms}, "cached": bool}."""
+    import torch
+    from . import evaluator as ev
+    lit = params.literal
+    level = lit.max_level if level is None else level
+    key = _cache_key(params, k, level)
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+        if key in cache:
+            set_tuning(params, **cache[key]["best"])
+            return dict(cache[key], cached=True)
+    if operands is None:
+        g = np.random.default_rng(7)
+        qmin = min(min(lit.q), min(lit.p))
+        nQ, nP, N = len(lit.q), len(lit.p), lit.n
+        beta = (nQ + nP - 1) // nP
+        kimg = g.integers(0, qmin, size=(beta, 2, nQ + nP, N), dtype=np.uint64)
+        E = ev.MKFEvaluator(params, ev.MKFKeySet(params, [kimg] * k, kimg))
+        cts = [ev.Ciphertext.from_array(params, g.integers(0, qmin, size=(k + 1, level + 1, N),
+                                                           dtype=np.uint64),
+                                        params.scheme == "ckks", scale=lit.scale) for _ in range(2)]
+        operands = (E, cts[0], cts[1])
+    E, left, right = operands
+    ckks = params.scheme == "ckks"
+    out = ev.Ciphertext(params, k + 1, E.output_level(left, right, ckks), ckks)
+    st = torch.cuda.Stream(device=params.device)
+    cs = ctypes.c_void_p(st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def time_fn(cnd):
+        set_tuning(params, **cnd)
+        E.MulRelin(left, right, out, rescale=ckks, materialize=True, stream=cs)  # warm-up
+        e0.record(st)
+        for _ in range(reps):
+            E.MulRelin(left, right, out, rescale=ckks, materialize=True, stream=cs)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    best, table = search(cands or candidates(), time_fn)
+    set_tuning(params, **best)
+    res = {"best": best, "ms": table, "cached": False}
+    if cache_path:
+        cache = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
+        cache[key] = {"best": best, "ms": table}
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return res

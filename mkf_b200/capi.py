@@ -68,6 +68,10 @@ class Job(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("fuse_ip", ctypes.c_int), ("ip_block", ctypes.c_int), ("modup_chunk", ctypes.c_int)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t),
                 ("slots", ctypes.c_int), ("queue_cap", ctypes.c_int)]
@@ -154,6 +158,8 @@ def lib():
         "mkf_mkf_rotate": (i, [vp, vp, vp, ctypes.c_uint64, vp, vp]),
         "mkf_ct_copy": (i, [vp, vp, vp, vp]),
         "mkf_slot_const": (i, [vp, vp, u64p, i, vp, vp]),
+        "mkf_ctx_get_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
+        "mkf_ctx_set_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
         "mkf_server_create": (i, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "mkf_job_scratch": (i, [ctypes.POINTER(Job), ctypes.POINTER(sz)]),
         "mkf_server_submit": (i, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]),

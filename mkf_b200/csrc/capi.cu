@@ -798,6 +798,28 @@ mkf_status mkf_slot_const(mkf_ctx *ctx, const mkf_ct *in, const uint64_t *consts
     return s;
 }
 
+mkf_status mkf_ctx_get_tuning(const mkf_ctx *ctx, mkf_tuning *out) {
+    if (!ctx || !out) return MKF_ERR_INVALID_ARG;
+    out->fuse_ip = ctx->c.tune.fuse_ip;
+    out->ip_block = ctx->c.tune.ip_block;
+    out->modup_chunk = ctx->c.tune.modup_chunk;
+    return MKF_OK;
+}
+
+mkf_status mkf_ctx_set_tuning(mkf_ctx *ctx, const mkf_tuning *t) {
+    if (!ctx || !t) return MKF_ERR_INVALID_ARG;
+    if ((t->fuse_ip != 0 && t->fuse_ip != 1) ||
+        (t->ip_block != 128 && t->ip_block != 256 && t->ip_block != 512) ||
+        (t->modup_chunk != 8 && t->modup_chunk != 12 && t->modup_chunk != 24))
+        return fail(ctx, MKF_ERR_INVALID_ARG, "tuning values out of range");
+    cudaSetDevice(ctx->c.device);
+    cudaDeviceSynchronize(); // launches already queued keep their choices
+    ctx->c.tune.fuse_ip = t->fuse_ip;
+    ctx->c.tune.ip_block = t->ip_block;
+    ctx->c.tune.modup_chunk = t->modup_chunk;
+    return MKF_OK;
+}
+
 mkf_status mkf_kklss_keyset_create(mkf_ctx *ctx, const mkf_key *crs_u, mkf_kklss_keyset **out) {
     if (!ctx || !crs_u || !out) return MKF_ERR_INVALID_ARG;
     if (crs_u->kind != MKF_KEY_GADGET || crs_u->ctx != ctx)

@@ -137,7 +137,7 @@ static uint64_t bitrev(uint64_t x, int bits) {
 const char *const kProfNames[PK_COUNT] = {
     "ntt_fwd_col", "ntt_fwd_row", "ntt_fwd_full", "ntt_inv_row", "ntt_inv_col", "ntt_inv_full",
     "decompose", "keyswitch_ip", "modup", "moddown_combine", "tensor", "rescale", "elementwise",
-    "ntt_digits_col", "ntt_digits_row"};
+    "ntt_digits_col", "ntt_digits_row", "ntt_digits_row_ip"};
 
 int Profiler::begin(int kind, cudaStream_t st, double bytes) {
     std::lock_guard<std::mutex> g(mu);

@@ -28,7 +28,7 @@ struct ModUpTab {
 enum ProfKind : int {
     PK_NTT_FWD_COL, PK_NTT_FWD_ROW, PK_NTT_FWD_FULL, PK_NTT_INV_ROW, PK_NTT_INV_COL,
     PK_NTT_INV_FULL, PK_DECOMPOSE, PK_IP, PK_MODUP, PK_COMBINE, PK_TENSOR, PK_RESCALE,
-    PK_ELEMENTWISE, PK_DIGITS_COL, PK_DIGITS_ROW, PK_COUNT
+    PK_ELEMENTWISE, PK_DIGITS_COL, PK_DIGITS_ROW, PK_DIGITS_ROW_IP, PK_COUNT
 };
 extern const char *const kProfNames[PK_COUNT];
 
@@ -68,6 +68,14 @@ class Context {
     double scale = 0;
     uint64_t t = 0;
     int n1 = 0, n2 = 0; // NTT split: 2^n1 column stages, 2^n2 row stages
+
+    // Launch choices the autotuner may change (mkf_ctx_set_tuning); all of
+    // them compute the same words.
+    struct Tuning {
+        int fuse_ip = 0;       // inner products fused into the digits' row pass
+        int ip_block = 256;    // threads per block of the inner-product kernel
+        int modup_chunk = 12;  // target limbs per thread of the summed ModUp
+    } tune;
 
     int qidx(int i) const { return i; }
     int pidx(int i) const { return nQ + i; }

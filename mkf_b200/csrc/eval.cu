@@ -142,9 +142,10 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1;
     const int beta = c.beta_of(level, 1);
     const long long poly = (long long)L1 * N, qp = (long long)(L1 + nP) * N, kk = k;
-    // 1. gadget decomposition of every party component
+    // 1-2. gadget decomposition of every party component and the fold key
+    // inner products (fused into the digits' row pass where it applies)
+    OwnNtt own;
     if (!bfv) {
-        OwnNtt own;
         for (int s = 0; s < nops; ++s) {
             d2d2(f.coeff + s * kk * poly, poly, ops[s].data + ops[s].cs, ops[s].cs, poly, k, st);
             own.p[s] = ops[s].data + ops[s].cs;
@@ -152,13 +153,35 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
         }
         own.split = k;
         ntt_inverse(c, lsq(f.coeff, poly, L1), nops * k, st);
-        decompose_ntt(c, f.coeff, poly, 0, level, 1, beta, f.dig, nops * k, f.dscr, st, &own);
-    } else {
-        for (int s = 0; s < nops; ++s)
-            decompose_ntt(c, ops[s].data + ops[s].cs, ops[s].cs, 0, level, 1, beta,
-                          f.dig + s * kk * beta * qp, k, f.dscr, st);
     }
-    // 2. fold key inner products: each key read once for every operand
+    bool fused = false;
+    if (c.tune.fuse_ip && (!bfv || nops == 1)) {
+        DigitIpArgs g;
+        g.groups = k;
+        g.nin = nops;
+        for (int i = 0; i < k; ++i) g.kptr[i] = fold.p[i];
+        g.k_tstride = 2LL * (nQ + nP) * N;
+        g.k_ostride = (long long)(nQ + nP) * N;
+        g.k_qlimbs = nQ;
+        g.out = f.acc;
+        g.out_gstride = 2 * nops * qp;
+        g.out_istride = 2 * qp;
+        g.out_ostride = qp;
+        if (!bfv)
+            fused = decompose_ntt_ip(c, f.coeff, poly, level, beta, f.dig, nops * k, f.dscr, g, st, &own);
+        else
+            fused = decompose_ntt_ip(c, ops[0].data + ops[0].cs, ops[0].cs, level, beta, f.dig, k,
+                                     f.dscr, g, st);
+    }
+    if (!fused) {
+        if (!bfv) {
+            decompose_ntt(c, f.coeff, poly, 0, level, 1, beta, f.dig, nops * k, f.dscr, st, &own);
+        } else {
+            for (int s = 0; s < nops; ++s)
+                decompose_ntt(c, ops[s].data + ops[s].cs, ops[s].cs, 0, level, 1, beta,
+                              f.dig + s * kk * beta * qp, k, f.dscr, st);
+        }
+    }
     IpArgs ip;
     ip.A = f.dig;
     ip.a_tstride = qp;
@@ -179,7 +202,7 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     ip.groups = k;
     ip.L1 = L1;
     ip.nP = nP;
-    launch_ip(c, ip, st);
+    if (!fused) launch_ip(c, ip, st);
     // 3. ModDown summed over parties, then the fold
     if (!bfv)
         ntt_inverse(c, lsp_of_qp(c, f.acc, qp, L1), 2 * nops * k, st);
@@ -410,15 +433,29 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         }
     }
     // relinearization key switch of mu2 (coefficient domain input)
+    bool rfused;
     {
         OwnNtt own;
         own.p[0] = mu2;
         own.pstride[0] = poly;
         own.split = 1;
-        decompose_ntt(c, bfv ? mu2 : rcoef, poly, 0, level, 1, beta, rdig, 1, dscr, st,
-                      bfv ? nullptr : &own);
+        DigitIpArgs g;
+        g.groups = 1;
+        g.nin = 1;
+        g.B = relin;
+        g.k_tstride = 2LL * (nQ + nP) * N;
+        g.k_ostride = (long long)(nQ + nP) * N;
+        g.k_qlimbs = nQ;
+        g.out = racc;
+        g.out_ostride = qp;
+        rfused = c.tune.fuse_ip &&
+                 decompose_ntt_ip(c, bfv ? mu2 : rcoef, poly, level, beta, rdig, 1, dscr, g, st,
+                                  bfv ? nullptr : &own);
+        if (!rfused)
+            decompose_ntt(c, bfv ? mu2 : rcoef, poly, 0, level, 1, beta, rdig, 1, dscr, st,
+                          bfv ? nullptr : &own);
     }
-    {
+    if (!rfused) {
         IpArgs r;
         r.A = rdig;
         r.a_tstride = qp;

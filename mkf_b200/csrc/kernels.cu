@@ -172,11 +172,41 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     ntt_forward_digits(c, src, out, npolys, st);
 }
 
+bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride, int level,
+                      int ndigits, uint64_t *dig, int npolys, uint64_t *scratch,
+                      const DigitIpArgs &ip, cudaStream_t st, const OwnNtt *own) {
+    if (c.n2 == 0 || c.logN < 13) return false;
+    if (ndigits <= 0 || npolys <= 0) return true;
+    const int alpha = c.alpha_of(1);
+    const size_t n = (size_t)npolys * ndigits * c.N;
+    uint64_t *y = scratch;
+    uint8_t *v = reinterpret_cast<uint8_t *>(scratch + n * alpha);
+    if (alpha >= 2) {
+        ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
+        note_launch();
+        digits_prep_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(
+            in, in_pstride, c.d_decomp[0], c.d_mods, y, v, level, alpha, ndigits, c.N);
+    }
+    DigitSrc src;
+    src.x = in;
+    src.x_pstride = in_pstride;
+    src.y = y;
+    src.v = v;
+    src.tabs = c.d_decomp[0];
+    src.ndigits = ndigits;
+    src.alpha = alpha;
+    src.level = level;
+    src.nQ = c.nQ;
+    if (own) src.own = *own;
+    ntt_forward_digits_ip(c, src, dig, npolys, ip, st);
+    return true;
+}
+
 // ----------------------------------------------------------------------------
 // inner products
 // ----------------------------------------------------------------------------
 template <int NIN, int NOUT>
-__global__ void __launch_bounds__(kBlock) ip_kernel(IpArgs a, const DevModulus *mods, int N,
+__global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mods, int N,
                                                      int pmod0) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= N) return;
@@ -222,7 +252,8 @@ __global__ void __launch_bounds__(kBlock) ip_kernel(IpArgs a, const DevModulus *
 
 void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
     if (a.groups <= 0 || a.nterms < 0) return;
-    dim3 grid = grid_for(c.N, a.L1 + a.nP, a.groups);
+    const int blk = c.tune.ip_block;
+    dim3 grid((c.N + blk - 1) / blk, a.L1 + a.nP, a.groups);
     const int pm = c.pidx(0);
     // algorithmic bytes: every digit word and key word read once, outputs written once
     const double lim = 8.0 * c.N * (a.L1 + a.nP);
@@ -233,13 +264,13 @@ void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
     ProfScope ps(c, PK_IP, st, bytes);
     note_launch();
     if (a.nin == 1 && a.nout == 1)
-        ip_kernel<1, 1><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+        ip_kernel<1, 1><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
     else if (a.nin == 1 && a.nout == 2)
-        ip_kernel<1, 2><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+        ip_kernel<1, 2><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
     else if (a.nin == 2 && a.nout == 2)
-        ip_kernel<2, 2><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+        ip_kernel<2, 2><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
     else if (a.nin == 2 && a.nout == 1)
-        ip_kernel<2, 1><<<grid, kBlock, 0, st>>>(a, c.d_mods, c.N, pm);
+        ip_kernel<2, 1><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
 }
 
 // ----------------------------------------------------------------------------
@@ -296,9 +327,8 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
 }
 
 // Summed ModUp: a thread owns one coefficient of one output polynomial and a
-// chunk of kSumChunk target limbs, and walks the terms, reconstructing each
-// term's y_i and correction once per chunk.
-constexpr int kSumChunk = 12;
+// chunk of CH target limbs, and walks the terms, reconstructing each term's
+// y_i and correction once per chunk.
 
 struct ModUpSumArgs {
     ModUpTab tab;
@@ -311,15 +341,15 @@ struct ModUpSumArgs {
     int row0, nt, N, terms, nchunks;
 };
 
-template <int MAXNS>
+template <int MAXNS, int CH>
 __global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.N) return;
-    const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * kSumChunk;
-    const int nj = min(kSumChunk, a.nt - j0);
-    uint64_t acc[kSumChunk];
+    const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * CH;
+    const int nj = min(CH, a.nt - j0);
+    uint64_t acc[CH];
 #pragma unroll
-    for (int jj = 0; jj < kSumChunk; ++jj) acc[jj] = 0;
+    for (int jj = 0; jj < CH; ++jj) acc[jj] = 0;
     for (int t = 0; t < a.terms; ++t) {
         const uint64_t *src = a.src + (long long)t * a.src_tstride + (long long)p * a.src_pstride;
         uint64_t xs[MAXNS], y[MAXNS];
@@ -328,7 +358,7 @@ __global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a) {
             if (i < a.tab.ns) xs[i] = src[(long long)i * a.N + x];
         const uint64_t v = reconstruct<MAXNS>(xs, a.tab, a.mods, y);
 #pragma unroll
-        for (int jj = 0; jj < kSumChunk; ++jj) {
+        for (int jj = 0; jj < CH; ++jj) {
             if (jj < nj) {
                 const DevModulus &m = a.mods[a.tgt(j0 + jj)];
                 acc[jj] = add_mod(acc[jj], canon(multsum<MAXNS>(y, a.tab, a.row0 + j0 + jj, v, m), m.q),
@@ -338,7 +368,7 @@ __global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a) {
     }
     uint64_t *out = a.out + (long long)p * a.out_pstride + (long long)j0 * a.N + x;
 #pragma unroll
-    for (int jj = 0; jj < kSumChunk; ++jj)
+    for (int jj = 0; jj < CH; ++jj)
         if (jj < nj) out[(long long)jj * a.N] = acc[jj];
 }
 
@@ -347,22 +377,32 @@ void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src
                       long long out_pstride, int row0, int nt, ModMap tgt, int npolys,
                       cudaStream_t st) {
     if (npolys <= 0 || nt <= 0) return;
-    const int nchunks = (nt + kSumChunk - 1) / kSumChunk;
+    const int ch = c.tune.modup_chunk;
+    const int nchunks = (nt + ch - 1) / ch;
     ModUpSumArgs a{tab, src, src_pstride, src_tstride, out, out_pstride, c.d_mods, tgt,
                    row0, nt, c.N, terms, nchunks};
     ProfScope ps(c, PK_MODUP, st, 8.0 * c.N * npolys * ((double)tab.ns * terms + nt));
     const dim3 grid = grid_for(c.N, npolys * nchunks);
     note_launch();
-    if (tab.ns <= 4)
-        modup_sum_kernel<4><<<grid, kBlock, 0, st>>>(a);
-    else if (tab.ns <= 8)
-        modup_sum_kernel<8><<<grid, kBlock, 0, st>>>(a);
-    else if (tab.ns <= 16)
-        modup_sum_kernel<16><<<grid, kBlock, 0, st>>>(a);
-    else if (tab.ns <= 32)
-        modup_sum_kernel<32><<<grid, kBlock, 0, st>>>(a);
-    else
-        modup_sum_kernel<64><<<grid, kBlock, 0, st>>>(a);
+#define MKF_SUM_NS(CH)                                                                             \
+    if (tab.ns <= 4)                                                                               \
+        modup_sum_kernel<4, CH><<<grid, kBlock, 0, st>>>(a);                                        \
+    else if (tab.ns <= 8)                                                                          \
+        modup_sum_kernel<8, CH><<<grid, kBlock, 0, st>>>(a);                                        \
+    else if (tab.ns <= 16)                                                                         \
+        modup_sum_kernel<16, CH><<<grid, kBlock, 0, st>>>(a);                                       \
+    else if (tab.ns <= 32)                                                                         \
+        modup_sum_kernel<32, CH><<<grid, kBlock, 0, st>>>(a);                                       \
+    else                                                                                           \
+        modup_sum_kernel<64, CH><<<grid, kBlock, 0, st>>>(a);
+    if (ch == 8) {
+        MKF_SUM_NS(8)
+    } else if (ch == 24) {
+        MKF_SUM_NS(24)
+    } else {
+        MKF_SUM_NS(12)
+    }
+#undef MKF_SUM_NS
 }
 
 // ----------------------------------------------------------------------------

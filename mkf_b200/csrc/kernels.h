@@ -37,6 +37,14 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
                    int level, int gamma, int ndigits, uint64_t *out, int npolys,
                    uint64_t *scratch, cudaStream_t st, const OwnNtt *own = nullptr);
 
+// decompose_ntt (gamma = 1) followed by the inner product fused into the
+// digits' row pass (DigitIpArgs; dig receives the column-pass output, its
+// row pass happens in registers).  Returns false (and does nothing) where the
+// fused path does not apply (logN < 13): use decompose_ntt + launch_ip.
+bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride, int level,
+                      int ndigits, uint64_t *dig, int npolys, uint64_t *scratch,
+                      const DigitIpArgs &ip, cudaStream_t st, const OwnNtt *own = nullptr);
+
 // Inner products of digit polynomials with key polynomials (Montgomery: B in
 // MForm):
 //   out[g][i][o][l] (+)= sum_t A[g][i][t][l] (.) B[g][t][o][l]

@@ -347,9 +347,13 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
 }
 
 // The butterfly passes of a forward phase on the tile in shared memory.
-template <int LOGS, bool LAZY>
-MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t) {
+// KEEP: the last pass leaves its 8 words in vout (thread t of column c then
+// holds points 8t..8t+7 of its sub-transform) instead of storing them.
+template <int LOGS, bool LAZY, bool KEEP = false>
+MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
+                        uint64_t *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    static_assert(pass_pos<LOGS>(NP - 1) == 0, "the last pass holds consecutive points");
     uint64_t v[8];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
@@ -371,9 +375,14 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t) {
                 }
             }
         }
+        if (KEEP && p == NP - 1) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = v[r];
-        __syncwarp();
+            for (int r = 0; r < 8; ++r) vout[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = v[r];
+            __syncwarp();
+        }
     }
 }
 
@@ -458,7 +467,9 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     const int mode = ns == 1 ? 0 : own_limb ? 1 : 2;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
     if (own_limb && src.own.p[0]) {
-        // the digit's own limb is the input limb itself: copy its NTT form
+        // the digit's own limb is the input limb itself: copy its NTT form,
+        // unless the fused row pass reads it from the input directly
+        if (src.own_skip) return;
         const int gp = src.poly0 + poly;
         const uint64_t *xn = (gp < src.own.split
                                   ? src.own.p[0] + (long long)gp * src.own.pstride[0]
@@ -686,7 +697,170 @@ template <typename K> static void digits_smem_attr(K kernel, int device) {
     done.insert(key);
 }
 
+// Dynamic shared memory of the fused row pass: the NTT tile and two
+// accumulator tiles.
+constexpr size_t kRowIpSmem = 3 * kTile * sizeof(uint64_t);
+
+// Row pass of the gadget digits fused with the key-switch inner product
+// (KeyswitchHoistedNoModDown, common.go:79-107): for one limb tile of one
+// polynomial (group g, input s), every digit is transformed in turn and its
+// words, still in registers after the last radix-8 pass, are multiplied by
+// the digit's two key polynomials and accumulated.  A digit's own limbs are
+// read from the NTT-domain input instead.  MRed(v, key) = v*key*2^-64 mod q
+// is canonical for any 64-bit v, so the lazy NTT outputs need no reduction,
+// and the sum equals the stand-alone inner product's exactly.
+template <int LOGS>
+__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a, DigitIpArgs g) {
+    constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
+    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t *s = dsm;
+    const int l = blockIdx.y;
+    const int grp = blockIdx.z % g.groups, sidx = blockIdx.z / g.groups;
+    const int poly = sidx * g.groups + grp;
+    const int m = a.ls.mod_of(l);
+    const DevModulus md = a.mods[m];
+    const uint64_t q = md.q;
+    const bool lazy = q < kLazyBound;
+    const int N = 1 << a.logN, R = 1 << a.n2;
+    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const long long base = (long long)blockIdx.x * kTile + c * S + 8 * t;
+    uint64_t *acc0 = dsm + kTile + c * S + 8 * t;
+    uint64_t *acc1 = acc0 + kTile;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) acc0[r] = acc1[r] = 0;
+    const uint64_t *kb = g.kptr[grp] ? g.kptr[grp] : g.B + (long long)grp * g.k_gstride;
+    const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N;
+    const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+    for (int d = 0; d < g.beta; ++d) {
+        const int start = d * g.alpha;
+        const bool own = g.own.p[0] && l < g.L1 && l >= start &&
+                         l < start + digit_ns(g.level, g.alpha, d);
+        uint64_t v[8];
+        if (own) {
+            const uint64_t *xn = (poly < g.own.split
+                                      ? g.own.p[0] + (long long)poly * g.own.pstride[0]
+                                      : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
+                                 (long long)l * N + base;
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(xn + r);
+                v[r] = w.x;
+                v[r + 1] = w.y;
+            }
+        } else {
+            const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N;
+            __syncthreads(); // the previous digit's tile is consumed
+            tile_load<LOGS, false>(s, src, R, tid);
+            __syncthreads();
+            if (lazy)
+                fwd_passes<LOGS, true, true>(s, tw, q, c, t, v);
+            else
+                fwd_passes<LOGS, false, true>(s, tw, q, c, t, v);
+        }
+        const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow + base;
+        const uint64_t *k1 = k0 + g.k_ostride;
+#pragma unroll
+        for (int r = 0; r < 8; r += 2) {
+            const ulonglong2 x0 = __ldg(reinterpret_cast<const ulonglong2 *>(k0 + r));
+            const ulonglong2 x1 = __ldg(reinterpret_cast<const ulonglong2 *>(k1 + r));
+            acc0[r] = add_mod(acc0[r], mred(v[r], x0.x, q, md.qinv), q);
+            acc0[r + 1] = add_mod(acc0[r + 1], mred(v[r + 1], x0.y, q, md.qinv), q);
+            acc1[r] = add_mod(acc1[r], mred(v[r], x1.x, q, md.qinv), q);
+            acc1[r + 1] = add_mod(acc1[r + 1], mred(v[r + 1], x1.y, q, md.qinv), q);
+        }
+    }
+    uint64_t *o0 = g.out + (long long)grp * g.out_gstride + (long long)sidx * g.out_istride +
+                   (long long)l * N + base;
+    uint64_t *o1 = o0 + g.out_ostride;
+#pragma unroll
+    for (int r = 0; r < 8; r += 2) {
+        *reinterpret_cast<ulonglong2 *>(o0 + r) = make_ulonglong2(acc0[r], acc0[r + 1]);
+        *reinterpret_cast<ulonglong2 *>(o1 + r) = make_ulonglong2(acc1[r], acc1[r + 1]);
+    }
+}
+
+template <typename K> static void smem_attr(K kernel, int device, size_t bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), device);
+    if (done.count(key)) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done.insert(key);
+}
+
+void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig, int npolys,
+                           const DigitIpArgs &ip0, cudaStream_t st) {
+    const int L1 = src0.level + 1, limbs = L1 + c.nP;
+    const int np = npolys * src0.ndigits;
+    if (np <= 0) return;
+    NttArgs a;
+    a.ls = LimbSet{dig, (long long)limbs * c.N, limbs, L1, 0, c.pidx(0)};
+    a.mods = c.d_mods;
+    a.logN = c.logN;
+    a.n1 = c.n1;
+    a.n2 = c.n2;
+    a.tw1 = c.d_fwd1;
+    a.tw2 = c.d_fwd2;
+    DigitSrc src = src0;
+    src.own_skip = src.own.p[0] != nullptr;
+    DigitIpArgs ip = ip0;
+    ip.dig = dig;
+    ip.dig_pstride = (long long)limbs * c.N;
+    ip.own = src.own;
+    ip.beta = src.ndigits;
+    ip.alpha = src.alpha;
+    ip.level = src.level;
+    ip.L1 = L1;
+    const int own = src.own.p[0] ? std::min(src.alpha, L1) : 0;
+    const double bytes_col = (double)c.N * np * (8.0 * (limbs - own) + 8.0 * src.alpha + 1.0);
+    // the fused row pass reads every transformed limb, each key word once per
+    // input, and writes the two accumulators
+    const double bytes_row = 8.0 * c.N * ((double)np * limbs +
+                                          (double)ip.groups * ip.nin * src.ndigits * 2 * limbs +
+                                          (double)ip.groups * ip.nin * 2 * limbs);
+    dim3 block(kPhaseThreads);
+    // the column pass: split at whole polynomials so that grid.y stays below 2^16
+    const int max_polys = std::max(src.ndigits, (65535 / limbs) / src.ndigits * src.ndigits);
+    note_launch(1);
+    switch (c.logN) {
+#define MKF_DIGITS_IP_CASE(LN, L1G, L2G)                                                           \
+    case LN: {                                                                                     \
+        for (int p0 = 0; p0 < np; p0 += max_polys) {                                               \
+            const int npp = std::min(max_polys, np - p0);                                          \
+            NttArgs b = a;                                                                         \
+            b.ls.base = dig + (long long)p0 * a.ls.poly_stride;                                    \
+            DigitSrc sb = src;                                                                     \
+            const int first_poly = p0 / src.ndigits;                                               \
+            sb.x = src.x + (long long)first_poly * src.x_pstride;                                  \
+            sb.y = src.y + (long long)p0 * src.alpha * c.N;                                        \
+            sb.v = src.v + (long long)p0 * c.N;                                                    \
+            sb.poly0 = first_poly;                                                                 \
+            dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs);                                     \
+            ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
+            smem_attr(ntt_fwd_digits_col<L1G>, c.device, kDigitsSmem);                             \
+            ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
+            if (p0) note_launch(1);                                                                \
+        }                                                                                          \
+        dim3 g2((1 << L1G) / (kTile >> L2G), limbs, ip.groups * ip.nin);                           \
+        ProfScope ps(c, PK_DIGITS_ROW_IP, st, bytes_row);                                          \
+        smem_attr(ntt_digits_row_ip<L2G>, c.device, kRowIpSmem);                                   \
+        note_launch(1);                                                                            \
+        ntt_digits_row_ip<L2G><<<g2, block, kRowIpSmem, st>>>(a, ip);                              \
+        break;                                                                                     \
+    }
+        MKF_DIGITS_IP_CASE(13, 6, 7)
+        MKF_DIGITS_IP_CASE(14, 7, 7)
+        MKF_DIGITS_IP_CASE(15, 7, 8)
+        MKF_DIGITS_IP_CASE(16, 8, 8)
+#undef MKF_DIGITS_IP_CASE
+    default: break;
+    }
+}
+
 void ntt_prepare(const Context &c) {
+    smem_attr(ntt_digits_row_ip<7>, c.device, kRowIpSmem);
+    smem_attr(ntt_digits_row_ip<8>, c.device, kRowIpSmem);
     digits_smem_attr(ntt_fwd_digits_col<6>, c.device);
     digits_smem_attr(ntt_fwd_digits_col<7>, c.device);
     digits_smem_attr(ntt_fwd_digits_col<8>, c.device);

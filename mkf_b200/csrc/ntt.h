@@ -32,7 +32,31 @@ struct DigitSrc {
     int ndigits = 0, alpha = 0, level = 0, nQ = 0;
     OwnNtt own;    // optional
     int poly0 = 0; // index of the first polynomial of this launch in `own`
+    int own_skip = 0; // own limbs are neither copied nor transformed
 };
+
+// Inner product fused into the digits' row pass (ntt_forward_digits_ip):
+// out[g][s][o][l] = sum_d NTT(digit d of poly s*groups+g)[l] (.) key_g[d][o][l]
+// (Montgomery products, keys in MForm), o = 0, 1.  Key of group g at
+// kptr[g] (or B + g*k_gstride), digit d at +d*k_tstride, output o at
+// +o*k_ostride, limb l at l*N (Q) or (k_qlimbs + l - L1)*N (P).
+struct DigitIpArgs {
+    const uint64_t *dig = nullptr; // filled by ntt_forward_digits_ip
+    long long dig_pstride = 0;
+    OwnNtt own;
+    int beta = 0, alpha = 0, level = 0, L1 = 0;
+    int groups = 1, nin = 1;
+    const uint64_t *kptr[64] = {};
+    const uint64_t *B = nullptr;
+    long long k_gstride = 0, k_tstride = 0, k_ostride = 0;
+    int k_qlimbs = 0;
+    uint64_t *out = nullptr;
+    long long out_gstride = 0, out_istride = 0, out_ostride = 0;
+};
+// Column pass of the digits (as ntt_forward_digits) then the fused row pass
+// + inner product; logN 13..16.  dig receives the column-pass output.
+void ntt_forward_digits_ip(const Context &c, const DigitSrc &src, uint64_t *dig, int npolys,
+                           const DigitIpArgs &ip, cudaStream_t st);
 // NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load.
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
                         cudaStream_t st);

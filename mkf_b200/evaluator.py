@@ -34,6 +34,7 @@ class Parameters:
         L = capi.lib()
         self.literal = literal
         self.scheme = scheme.lower()
+        self.device = device
         self._q = np.array(literal.q, dtype=np.uint64)
         self._p = np.array(literal.p, dtype=np.uint64)
         self._qm = np.array(literal.q_mul or (0,), dtype=np.uint64)
