@@ -224,18 +224,36 @@ __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mod
     for (int i = 0; i < NIN; ++i)
 #pragma unroll
         for (int o = 0; o < NOUT; ++o) acc[i][o].zero();
-    for (int t = 0; t < a.nterms; ++t) {
-        uint64_t bv[NOUT];
+    // terms in groups of TB: all loads of a group are issued before its MACs
+    constexpr int TB = 3;
+    auto load = [&](int t, uint64_t *bv, uint64_t *av) {
         const uint64_t *bp = (a.bptr_per_term ? a.bptr[t] : Bg) + boff +
                              (a.bptr_per_term ? 0 : (long long)t * a.b_tstride);
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) bv[o] = bp[(long long)o * a.b_ostride];
+        for (int o = 0; o < NOUT; ++o) bv[o] = __ldg(bp + (long long)o * a.b_ostride);
 #pragma unroll
-        for (int i = 0; i < NIN; ++i) {
-            const uint64_t av = a.A[aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride];
+        for (int i = 0; i < NIN; ++i)
+            av[i] = __ldg(a.A + aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride);
+    };
+    int t = 0;
+    for (; t + TB <= a.nterms; t += TB) {
+        uint64_t bv[TB][NOUT], av[TB][NIN];
 #pragma unroll
-            for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av, bv[o], m.q);
-        }
+        for (int u = 0; u < TB; ++u) load(t + u, bv[u], av[u]);
+#pragma unroll
+        for (int u = 0; u < TB; ++u)
+#pragma unroll
+            for (int i = 0; i < NIN; ++i)
+#pragma unroll
+                for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av[u][i], bv[u][o], m.q);
+    }
+    for (; t < a.nterms; ++t) {
+        uint64_t bv[NOUT], av[NIN];
+        load(t, bv, av);
+#pragma unroll
+        for (int i = 0; i < NIN; ++i)
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av[i], bv[o], m.q);
     }
 #pragma unroll
     for (int i = 0; i < NIN; ++i)
