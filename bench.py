@@ -421,6 +421,61 @@ def run_gpu(a):
                "h2d_bytes_per_step": 2 * a.batch * words_in * 8,
                "d2h_bytes_per_step": a.batch * words_out * 8}
 
+    # the same workload at level 8 (L1 = 9 limbs, beta = 3): plain and batched
+    lvl8 = None
+    if level > 8:
+        l8 = 8
+        ins8 = [(ev.Ciphertext.from_array(P, random_limbs(g, lit.q[: l8 + 1], N, k + 1), True,
+                                          scale=lit.scale),
+                 ev.Ciphertext.from_array(P, random_limbs(g, lit.q[: l8 + 1], N, k + 1), True,
+                                          scale=lit.scale)) for _ in range(nin)]
+        lo8 = E.output_level(ins8[0][0], ins8[0][1], True)
+        outs8 = [ev.Ciphertext(P, k + 1, lo8, True) for _ in range(nin)]
+
+        def product8(i, s):
+            l, r = ins8[i % nin]
+            E.MulRelin(l, r, outs8[i % nin], rescale=True, materialize=True, stream=ctypes_stream(s))
+
+        for i in range(a.warmup):
+            product8(i, s0)
+        barrier()
+        lat8 = []
+        for i in range(plain_steps):
+            ev0.record(s0)
+            product8(i, s0)
+            ev1.record(s0)
+            ev1.synchronize()
+            lat8.append(ev0.elapsed_time(ev1))
+        barrier()
+
+        def batched8(step):
+            start = torch.cuda.Event()
+            start.record(streams[0])
+            for s in streams[1:]:
+                s.wait_event(start)
+            for j in range(a.batch):
+                product8(step * a.batch + j, streams[j % len(streams)])
+            for s in streams[1:]:
+                e = torch.cuda.Event()
+                e.record(s)
+                streams[0].wait_event(e)
+
+        for i in range(a.warmup):
+            batched8(i)
+        barrier()
+        t0.record(streams[0])
+        for step in range(a.steps):
+            batched8(step)
+        t1.record(streams[0])
+        t1.synchronize()
+        barrier()
+        ms8 = max_over_ranks(t0.elapsed_time(t1))
+        lat8.sort()
+        lvl8 = {"level": l8, "plain": ws * plain_steps / (max_over_ranks(sum(lat8)) / 1e3),
+                "batched": ws * a.steps * a.batch / (ms8 / 1e3), "unit": "mult+relin ops/s",
+                "latency_ms": {"p50": lat8[len(lat8) // 2],
+                               "p99": lat8[min(len(lat8) - 1, int(0.99 * len(lat8)))]}}
+
     mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
     serve = run_serve(a, local, rank) if a.serve_seconds > 0 else None
 
@@ -447,6 +502,7 @@ def run_gpu(a):
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roofline,
+            "level8": lvl8,
             "autotune": {"best": tuned["best"],
                          "ms_per_product": tuned["ms"]},
             "batched_mix": mix,
