@@ -301,6 +301,11 @@ MKF_DEV Tw ldtw(const Tw *p) {
     const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2 *>(p));
     return Tw{v.x, v.y};
 }
+// twiddle read from shared memory (staged tables)
+MKF_DEV Tw ldtw_s(const Tw *p) {
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
+    return Tw{v.x, v.y};
+}
 
 template <int LOGS, bool COLS>
 MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid) {
@@ -349,7 +354,7 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
 // The butterfly passes of a forward phase on the tile in shared memory.
 // KEEP: the last pass leaves its 8 words in vout (thread t of column c then
 // holds points 8t..8t+7 of its sub-transform) instead of storing them.
-template <int LOGS, bool LAZY, bool KEEP = false>
+template <int LOGS, bool LAZY, bool KEEP = false, bool TWS = false>
 MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
                         uint64_t *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
@@ -368,10 +373,11 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
                     const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
+                    const Tw w = TWS ? ldtw_s(tw + (1 << st) + i) : ldtw(tw + (1 << st) + i);
                     if (LAZY)
-                        ct_bfly_lazy(v[r], v[r + stride], ldtw(tw + (1 << st) + i), q);
+                        ct_bfly_lazy(v[r], v[r + stride], w, q);
                     else
-                        ct_bfly(v[r], v[r + stride], ldtw(tw + (1 << st) + i), q);
+                        ct_bfly(v[r], v[r + stride], w, q);
                 }
             }
         }
@@ -405,15 +411,53 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         if (l < a.ls.nq && l >= start && l < start + digit_ns(a.own_level, a.own_alpha, d)) return;
     }
     tile_load<LOGS, COLS>(s, data, R, tid);
+    // the column pass stages its table (S entries, shared by every column) in
+    // shared memory; the row pass reads its per-row tables from global memory
+    // (staging the tile's C*S row twiddles measured slower)
+    extern __shared__ __align__(16) uint64_t twdyn[];
+    Tw *tws = reinterpret_cast<Tw *>(twdyn);
+    if (COLS) {
+        const ulonglong2 *twg = reinterpret_cast<const ulonglong2 *>(a.tw1 + (size_t)m * (1 << a.n1));
+        ulonglong2 *d = reinterpret_cast<ulonglong2 *>(tws);
+        for (int i = tid; i < S; i += kPhaseThreads) d[i] = __ldg(twg + i);
+    }
     __syncthreads();
-    const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
-                        : a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-    if (lazy)
-        fwd_passes<LOGS, true>(s, tw, q, c, t);
-    else
-        fwd_passes<LOGS, false>(s, tw, q, c, t);
+    if (COLS) {
+        if (lazy)
+            fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
+        else
+            fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
+    } else {
+        const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+        if (lazy)
+            fwd_passes<LOGS, true>(s, tw, q, c, t);
+        else
+            fwd_passes<LOGS, false>(s, tw, q, c, t);
+    }
     __syncthreads();
     tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedNone : lazy ? kRedAny : kRed4);
+}
+
+// Dynamic shared memory of ntt_fwd_phase: its staged twiddles.
+template <int LOGS, bool COLS> constexpr size_t fwd_phase_smem() {
+    return COLS ? (size_t(1) << LOGS) * sizeof(Tw) : 0;
+}
+
+template <typename K> static void smem_attr(K kernel, int device, size_t bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), device);
+    if (done.count(key)) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done.insert(key);
+}
+
+template <int LOGS, bool COLS>
+static void launch_fwd_phase(dim3 grid, cudaStream_t st, const NttArgs &b, int device) {
+    constexpr size_t sm = fwd_phase_smem<LOGS, COLS>();
+    smem_attr(ntt_fwd_phase<LOGS, COLS>, device, sm);
+    ntt_fwd_phase<LOGS, COLS><<<grid, kPhaseThreads, sm, st>>>(b);
 }
 
 MKF_DEV void cp_async16(void *smem, const void *gmem) {
@@ -434,7 +478,7 @@ MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
 
 // Dynamic shared memory of the digit column pass: the NTT tile, two staging
 // tiles for y_i and one byte per word for the float64 correction.
-constexpr size_t kDigitsSmem = 3 * kTile * sizeof(uint64_t) + kTile;
+constexpr size_t kDigitsSmem = 3 * kTile * sizeof(uint64_t) + kTile + 256 * sizeof(Tw);
 
 // Column pass of the NTT of gadget digits with the decomposition fused into
 // the load: every word of the tile is reconstructed from the digit's y_i and
@@ -452,6 +496,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     uint64_t *s = dsm;
     uint64_t *stg = dsm + kTile;
     uint8_t *vb = reinterpret_cast<uint8_t *>(dsm + 3 * kTile);
+    Tw *tws = reinterpret_cast<Tw *>(dsm + 3 * kTile + kTile / 8); // the column table, staged
     __shared__ uint64_t tq[8], tv[9];
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y / limbs, l = blockIdx.y % limbs;
@@ -483,6 +528,11 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
             dst[coef] = xn[coef];
         }
         return;
+    }
+    {
+        const uint64_t *src = reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * (1 << a.n1));
+        uint64_t *dst = reinterpret_cast<uint64_t *>(tws);
+        for (int i = tid; i < 2 * S; i += kPhaseThreads) dst[i] = src[i];
     }
     if (mode == 2) {
         if (tid < 2 * ns + 1) {
@@ -544,9 +594,9 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     }
     __syncthreads();
     if (q < kLazyBound)
-        fwd_passes<LOGS, true>(s, a.tw1 + (size_t)m * (1 << a.n1), q, c, t);
+        fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
     else
-        fwd_passes<LOGS, false>(s, a.tw1 + (size_t)m * (1 << a.n1), q, c, t);
+        fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
     __syncthreads();
     uint64_t *data = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N;
     tile_store<LOGS, true>(s, data, R, tid, md, kRedNone);
@@ -639,10 +689,10 @@ static void launch_phases(const NttArgs &b, int np, int limbs, cudaStream_t st, 
     } else {
         {
             ProfScope ps(c, PK_NTT_FWD_COL, st, bytes);
-            ntt_fwd_phase<LOG1, true><<<g1, block, 0, st>>>(b);
+            launch_fwd_phase<LOG1, true>(g1, st, b, c.device);
         }
         ProfScope ps(c, PK_NTT_FWD_ROW, st, bytes);
-        ntt_fwd_phase<LOG2, false><<<g2, block, 0, st>>>(b);
+        launch_fwd_phase<LOG2, false>(g2, st, b, c.device);
     }
 }
 
@@ -779,16 +829,6 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     }
 }
 
-template <typename K> static void smem_attr(K kernel, int device, size_t bytes) {
-    static std::mutex mu;
-    static std::set<std::pair<const void *, int>> done;
-    std::lock_guard<std::mutex> g(mu);
-    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), device);
-    if (done.count(key)) return;
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    done.insert(key);
-}
-
 void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig, int npolys,
                            const DigitIpArgs &ip0, cudaStream_t st) {
     const int L1 = src0.level + 1, limbs = L1 + c.nP;
@@ -859,6 +899,11 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
 }
 
 void ntt_prepare(const Context &c) {
+    smem_attr(ntt_fwd_phase<6, true>, c.device, fwd_phase_smem<6, true>());
+    smem_attr(ntt_fwd_phase<7, true>, c.device, fwd_phase_smem<7, true>());
+    smem_attr(ntt_fwd_phase<8, true>, c.device, fwd_phase_smem<8, true>());
+    smem_attr(ntt_fwd_phase<7, false>, c.device, fwd_phase_smem<7, false>());
+    smem_attr(ntt_fwd_phase<8, false>, c.device, fwd_phase_smem<8, false>());
     smem_attr(ntt_digits_row_ip<7>, c.device, kRowIpSmem);
     smem_attr(ntt_digits_row_ip<8>, c.device, kRowIpSmem);
     digits_smem_attr(ntt_fwd_digits_col<6>, c.device);
@@ -915,7 +960,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
             ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
-        ntt_fwd_phase<L2G, false><<<g2, block, 0, st>>>(b);                                        \
+        launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \
         break;                                                                                     \
     }
             MKF_DIGITS_CASE(13, 6, 7)
