@@ -1,5 +1,5 @@
 // Shared device types and 64-bit modular arithmetic for the multi-key
-// mult+relin kernels (sm_100a, integer pipes only).
+// mult+relin kernels (sm_100a).
 //
 // Conventions follow the reference's arithmetic (Lattigo v2.3.0 as called
 // from software/kklss/mkrlwe and software/mkf/mkf_cpu): Montgomery
@@ -33,11 +33,17 @@ struct DevModulus {
     uint64_t last_sh;
     double qd;        // (double)q, as the reference's float64 correction uses
     uint64_t one_sh;  // floor(2^64 / q): Shoup companion of 1
+    double qinvd;     // 1/q rounded to double
 };
 
 // A twiddle with its Shoup companion, loaded as one 16-byte word.
 struct Tw {
     uint64_t w, ws;
+};
+
+// A twiddle of the float64 transform: w and w/q, both rounded to double.
+struct TwD {
+    double w, wq;
 };
 
 // A set of limbs to transform/process: npolys polynomials, each with
@@ -116,6 +122,49 @@ MKF_DEV uint64_t reduce4(uint64_t x, uint64_t q) {
     uint64_t t2 = 2 * q;
     x = x >= t2 ? x - t2 : x;
     return x >= q ? x - q : x;
+}
+
+// ---------------------------------------------------------------------------
+// Float64 residues for moduli below 2^50.  B200 issues a float64 fused
+// multiply-add at the rate of a 32-bit integer multiply, and a product modulo
+// q takes six float64 operations against about twenty integer multiply-pipe
+// slots for a 64-bit Shoup product, so the NTT of these limbs runs on the
+// float64 pipe.  Words are integers held exactly in doubles (|x| < 2^53);
+// every step below is exact, so the canonical results are those of the
+// integer arithmetic.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kFp64Bound = 1ull << 50;
+#define MKF_F_RND 6755399441055744.0 // 1.5 * 2^52: fma(a, b, RND) - RND = round(a*b), |a*b| < 2^51
+#define MKF_F_2P52 4503599627370496.0
+
+// v*w - k*q with k = round(v*w/q): h + l = v*w exactly (two-product), k from
+// wq = w/q (relative error 2^-53) is within 1/2 + |v|*2^-53 of v*w/q, and
+// h - k*q and its sum with l are integers below 2^53, hence exact.  Needs
+// |v| < 2^51; returns |r| <= (1/2 + |v|*2^-53) * q.
+MKF_DEV double mulmod_f(double v, double w, double wq, double q) {
+    const double h = __dmul_rn(v, w);
+    const double l = __fma_rn(v, w, -h);
+    const double k = __dadd_rn(__fma_rn(v, wq, MKF_F_RND), -MKF_F_RND);
+    return __dadd_rn(__fma_rn(-k, q, h), l);
+}
+// x - round(x/q)*q, |result| <= q/2 (plus a rounding unit of the quotient).
+MKF_DEV double reduce_f(double x, double qinv, double q) {
+    const double k = __dadd_rn(__fma_rn(x, qinv, MKF_F_RND), -MKF_F_RND);
+    return __fma_rn(-k, q, x);
+}
+// uint64 below 2^52 -> double
+MKF_DEV double u64_to_f(uint64_t v) {
+    return __dadd_rn(__longlong_as_double((long long)(v | 0x4330000000000000ull)), -MKF_F_2P52);
+}
+// canonical v in [0,q) -> the centered representative in (-q/2, q/2], as a double
+MKF_DEV double centered_f(uint64_t v, uint64_t q) {
+    const long long x = (long long)(v > (q >> 1) ? v - q : v);
+    return __dadd_rn(__longlong_as_double(x + 0x4338000000000000ll), -MKF_F_RND);
+}
+// |x| < q (an integer) -> canonical uint64 in [0,q)
+MKF_DEV uint64_t canon_f(double x, double q) {
+    const double y = __dadd_rn(x, x < 0.0 ? q + MKF_F_2P52 : MKF_F_2P52);
+    return (uint64_t)__double_as_longlong(y) - 0x4330000000000000ull;
 }
 
 // 128-bit accumulator with the high word kept below q, so that a final

@@ -303,6 +303,7 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         d.ninv = h_invmod((uint64_t)N, qq);
         d.ninv_sh = h_shoup(d.ninv, qq);
         d.qd = (double)qq;
+        d.qinvd = 1.0 / (double)qq;
         d.one_sh = h_shoup(1, qq);
         uint64_t g = h_primitive_root(qq);
         uint64_t psi = h_powmod(g, (qq - 1) / (2ull * N), qq);
@@ -343,6 +344,22 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
     if (n2) {
         d_fwd2 = upload(fwd2);
         d_inv2 = upload(inv2);
+    }
+    // float64 twiddles (w, w/q) for the limbs below 2^50; the tables cover
+    // every modulus so that they index like the integer ones
+    auto to_f = [&](const std::vector<Tw> &t, size_t per) {
+        std::vector<TwD> o(t.size());
+        for (size_t i = 0; i < t.size(); ++i) {
+            const double q = (double)all[i / per];
+            o[i] = TwD{(double)t[i].w, (double)t[i].w / q};
+        }
+        return o;
+    };
+    d_fwd1d = upload(to_f(fwd1, S1));
+    d_inv1d = upload(to_f(inv1, S1));
+    if (n2) {
+        d_fwd2d = upload(to_f(fwd2, N));
+        d_inv2d = upload(to_f(inv2, N));
     }
 
     // gadget decomposition tables (Q ring), gamma = 1 (Lattigo) and 2 (KKLSS)

@@ -84,6 +84,8 @@ class Context {
     // device tables
     DevModulus *d_mods = nullptr;
     Tw *d_fwd1 = nullptr, *d_fwd2 = nullptr, *d_inv1 = nullptr, *d_inv2 = nullptr;
+    // the same tables for the float64 transform of limbs below 2^50
+    TwD *d_fwd1d = nullptr, *d_fwd2d = nullptr, *d_inv1d = nullptr, *d_inv2d = nullptr;
 
     // decomposition tables, gamma in {1,2}: index [gamma-1][digit][ns]
     std::vector<ModUpTab> decomp_tabs[2];

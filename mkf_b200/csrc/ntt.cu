@@ -10,7 +10,9 @@
 // stages one 4096-word tile in shared memory through coalesced 128-byte
 // loads, runs its stages there, and writes back; the column pass leaves
 // values in [0,4q), the row pass finishes canonical.  The last inverse stage
-// folds in N^-1.  All products are Shoup products on the integer pipes.
+// folds in N^-1.  Products are Shoup products on the integer pipes, except
+// in the forward transform of limbs below 2^50, which runs on the float64
+// pipe (mulmod_f): the column pass hands the row pass centered doubles.
 #include "ntt.h"
 
 #include <mutex>
@@ -29,6 +31,8 @@ struct NttArgs {
     const DevModulus *mods;
     const Tw *tw1;
     const Tw *tw2;
+    const TwD *tw1d = nullptr; // float64 tables (limbs below 2^50)
+    const TwD *tw2d = nullptr;
     int logN, n1, n2;
     // row pass of gadget digits [poly][digit][limb]: skip each digit's own
     // limbs (already final, copied by the column pass); 0 = transform all
@@ -80,6 +84,17 @@ __device__ __forceinline__ void gs_bfly_lazy(uint64_t &U, uint64_t &V, const Tw 
     const uint64_t x = U + V;
     V = shoup_lazy4(U + bias - V, w.w, w.ws, q);
     U = x;
+}
+
+// Float64 Cooley-Tukey butterfly (mulmod_f): from |U|, |V| <= B*q the
+// outputs stay below (B + 1/2 + B/8) q for q < 2^50, so a radix-8 pass of
+// three stages that starts from centered words (B = 1/2) keeps every V
+// operand below 2q (the rounding trick's range) and ends below 2.5q.
+__device__ __forceinline__ void ct_bfly_f(double &U, double &V, const TwD w, double q) {
+    const double t = mulmod_f(V, w.w, w.wq, q);
+    const double u = U;
+    U = __dadd_rn(u, t);
+    V = __dadd_rn(u, -t);
 }
 
 // MODE 0: whole limb in one tile. MODE 1: column pass. MODE 2: row pass.
@@ -306,25 +321,43 @@ MKF_DEV Tw ldtw_s(const Tw *p) {
     const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
     return Tw{v.x, v.y};
 }
+MKF_DEV TwD ldtwd(const TwD *p) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return TwD{v.x, v.y};
+}
+MKF_DEV TwD ldtwd_s(const TwD *p) {
+    const double2 v = *reinterpret_cast<const double2 *>(p);
+    return TwD{v.x, v.y};
+}
 
-template <int LOGS, bool COLS>
-MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid) {
+// CONV: the words are integers below 2^52 that enter the float64 transform;
+// they are stored as the bits of their centered doubles.
+template <int LOGS, bool COLS, bool CONV = false>
+MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double qi = 0.0,
+                       double qd = 0.0) {
     constexpr int S = 1 << LOGS, C = kTile / S;
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const int idx = e * kPhaseThreads + tid;
+        uint64_t v;
+        int a;
         if (COLS) {
             const int r = idx / C, cc = idx % C;
-            s[saddr<S>(cc, r)] = data[blockIdx.x * C + r * R + cc];
+            a = saddr<S>(cc, r);
+            v = data[blockIdx.x * C + r * R + cc];
         } else {
             const int cc = idx / S, j = idx % S;
-            s[saddr<S>(cc, j)] = data[(long long)blockIdx.x * kTile + idx];
+            a = saddr<S>(cc, j);
+            v = data[(long long)blockIdx.x * kTile + idx];
         }
+        if (CONV) v = (uint64_t)__double_as_longlong(reduce_f(u64_to_f(v), qi, qd));
+        s[a] = v;
     }
 }
 
-// Store reductions: none, [0,4q) -> [0,q), any -> [0,q), any -> [0,2q).
-enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q };
+// Store reductions: none, [0,4q) -> [0,q), any -> [0,q), any -> [0,2q),
+// centered double -> [0,q).
+enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q, kRedF };
 
 template <int LOGS, bool COLS>
 MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const DevModulus &md,
@@ -347,6 +380,7 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
         if (red == kRed4) v = reduce4(v, md.q);
         else if (red == kRedAny) v = reduce_any(v, md.q, md.one_sh);
         else if (red == kRed2q) v = reduce_2q(v, md.q, md.one_sh);
+        else if (red == kRedF) v = canon_f(__longlong_as_double((long long)v), md.qd);
         data[o] = v;
     }
 }
@@ -392,6 +426,46 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
     }
 }
 
+// The passes of a forward phase in float64 (limbs below 2^50): the tile holds
+// the bits of centered doubles, and every pass ends by reducing its words to
+// |x| <= q/2, so that the next pass (or phase) starts centered again.  KEEP:
+// the last pass leaves its words in vout, centered.
+template <int LOGS, bool KEEP = false, bool TWS = false>
+MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c, int t,
+                          double *vout = nullptr) {
+    constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    double v[8];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const int st = 3 * p + u;
+            if (st < LOGS) {
+                const int stride = 1 << (LOGS - 1 - st - pass_pos<LOGS>(p));
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    if (r & stride) continue;
+                    const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
+                    const TwD w = TWS ? ldtwd_s(tw + (1 << st) + i) : ldtwd(tw + (1 << st) + i);
+                    ct_bfly_f(v[r], v[r + stride], w, q);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
+        if (KEEP && p == NP - 1) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) vout[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = (uint64_t)__double_as_longlong(v[r]);
+            __syncwarp();
+        }
+    }
+}
+
 template <int LOGS, bool COLS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
@@ -410,18 +484,36 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         const int d = (blockIdx.y / limbs) % a.own_ndigits, start = d * a.own_alpha;
         if (l < a.ls.nq && l >= start && l < start + digit_ns(a.own_level, a.own_alpha, d)) return;
     }
-    tile_load<LOGS, COLS>(s, data, R, tid);
+    // float64 limbs: the column pass converts the input words, the row pass
+    // reads the column pass's doubles and stores canonical words
+    const bool fp = q < kFp64Bound;
+    if (COLS && fp)
+        tile_load<LOGS, true, true>(s, data, R, tid, md.qinvd, md.qd);
+    else
+        tile_load<LOGS, COLS>(s, data, R, tid);
     // the column pass stages its table (S entries, shared by every column) in
     // shared memory; the row pass reads its per-row tables from global memory
     // (staging the tile's C*S row twiddles measured slower)
     extern __shared__ __align__(16) uint64_t twdyn[];
     Tw *tws = reinterpret_cast<Tw *>(twdyn);
     if (COLS) {
-        const ulonglong2 *twg = reinterpret_cast<const ulonglong2 *>(a.tw1 + (size_t)m * (1 << a.n1));
+        const ulonglong2 *twg =
+            fp ? reinterpret_cast<const ulonglong2 *>(a.tw1d + (size_t)m * (1 << a.n1))
+               : reinterpret_cast<const ulonglong2 *>(a.tw1 + (size_t)m * (1 << a.n1));
         ulonglong2 *d = reinterpret_cast<ulonglong2 *>(tws);
         for (int i = tid; i < S; i += kPhaseThreads) d[i] = __ldg(twg + i);
     }
     __syncthreads();
+    if (fp) {
+        if (COLS)
+            fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
+        else
+            fwd_passes_f<LOGS>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md.qd,
+                               md.qinvd, c, t);
+        __syncthreads();
+        tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedNone : kRedF);
+        return;
+    }
     if (COLS) {
         if (lazy)
             fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
@@ -529,8 +621,12 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         }
         return;
     }
+    // float64 limbs (below 2^50): the words enter the transform as centered
+    // doubles and leave it as doubles for the row pass
+    const bool fp = q < kFp64Bound;
     {
-        const uint64_t *src = reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * (1 << a.n1));
+        const uint64_t *src = fp ? reinterpret_cast<const uint64_t *>(a.tw1d + (size_t)m * (1 << a.n1))
+                                 : reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * (1 << a.n1));
         uint64_t *dst = reinterpret_cast<uint64_t *>(tws);
         for (int i = tid; i < 2 * S; i += kPhaseThreads) dst[i] = src[i];
     }
@@ -581,7 +677,8 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         for (int e = 0; e < 8; ++e) {
             const int idx = e * kPhaseThreads + tid;
             const uint64_t h = __umul64hi(lo[e] * md.qinv, q);
-            s[saddr<S>(idx % C, idx / C)] = canon3(hi[e] - h + q + tv[vb[idx]], q);
+            const uint64_t r = canon3(hi[e] - h + q + tv[vb[idx]], q);
+            s[saddr<S>(idx % C, idx / C)] = fp ? (uint64_t)__double_as_longlong(centered_f(r, q)) : r;
         }
     } else {
         const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)(mode == 0 ? start : l) * N;
@@ -589,11 +686,14 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         for (int e = 0; e < 8; ++e) {
             const int idx = e * kPhaseThreads + tid;
             const int r = idx / C, cc = idx % C;
-            s[saddr<S>(cc, r)] = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
+            const uint64_t x = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
+            s[saddr<S>(cc, r)] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
         }
     }
     __syncthreads();
-    if (q < kLazyBound)
+    if (fp)
+        fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
+    else if (q < kLazyBound)
         fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
     else
         fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
@@ -707,6 +807,8 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
     a.n2 = c.n2;
     a.tw1 = inverse ? c.d_inv1 : c.d_fwd1;
     a.tw2 = inverse ? c.d_inv2 : c.d_fwd2;
+    a.tw1d = inverse ? c.d_inv1d : c.d_fwd1d;
+    a.tw2d = inverse ? c.d_inv2d : c.d_fwd2d;
     // grid.y is limited to 65535: split the polynomial range if needed
     const int max_polys = std::max(1, 65535 / ls.limbs);
     for (int p0 = 0; p0 < npolys; p0 += max_polys) {
@@ -781,6 +883,8 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const uint64_t *kb = g.kptr[grp] ? g.kptr[grp] : g.B + (long long)grp * g.k_gstride;
     const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N;
     const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+    const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+    const bool fp = q < kFp64Bound;
     for (int d = 0; d < g.beta; ++d) {
         const int start = d * g.alpha;
         const bool own = g.own.p[0] && l < g.L1 && l >= start &&
@@ -802,7 +906,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
             __syncthreads(); // the previous digit's tile is consumed
             tile_load<LOGS, false>(s, src, R, tid);
             __syncthreads();
-            if (lazy)
+            if (fp) {
+                // centered doubles -> [0,q) words (MRed takes any 64-bit word)
+                double vf[8];
+                fwd_passes_f<LOGS, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[r] = canon_f(vf[r], md.qd);
+            } else if (lazy)
                 fwd_passes<LOGS, true, true>(s, tw, q, c, t, v);
             else
                 fwd_passes<LOGS, false, true>(s, tw, q, c, t, v);
@@ -842,6 +952,8 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
     a.n2 = c.n2;
     a.tw1 = c.d_fwd1;
     a.tw2 = c.d_fwd2;
+    a.tw1d = c.d_fwd1d;
+    a.tw2d = c.d_fwd2d;
     DigitSrc src = src0;
     src.own_skip = src.own.p[0] != nullptr;
     DigitIpArgs ip = ip0;
@@ -924,6 +1036,8 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
     a.n2 = c.n2;
     a.tw1 = c.d_fwd1;
     a.tw2 = c.d_fwd2;
+    a.tw1d = c.d_fwd1d;
+    a.tw2d = c.d_fwd2d;
     // split only at whole polynomials so that (poly, digit) stays derivable
     const int max_polys = std::max(src.ndigits, (65535 / limbs) / src.ndigits * src.ndigits);
     for (int p0 = 0; p0 < np; p0 += max_polys) {
