@@ -205,6 +205,10 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
     t.ns = (int)src.size();
     t.nt = (int)tgt.size();
     std::vector<uint64_t> inv(t.ns), qmod((size_t)t.nt * t.ns), vq((size_t)t.nt * (t.ns + 1));
+    std::vector<double> qmodd((size_t)t.nt * t.ns * 2);
+    t.fp_src = 1;
+    for (int i = 0; i < t.ns; ++i)
+        if (all[src[i]] >= kFp64Bound) t.fp_src = 0;
     for (int i = 0; i < t.ns; ++i) {
         uint64_t qi = all[src[i]], prod = 1;
         for (int j = 0; j < t.ns; ++j)
@@ -215,6 +219,8 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
             for (int j = 0; j < t.ns; ++j)
                 if (j != i) pr = h_mulmod(pr, all[src[j]] % pk, pk);
             qmod[(size_t)k * t.ns + i] = h_mform(pr, pk);
+            qmodd[((size_t)k * t.ns + i) * 2] = (double)pr;
+            qmodd[((size_t)k * t.ns + i) * 2 + 1] = (double)pr / (double)pk;
         }
     }
     for (int k = 0; k < t.nt; ++k) {
@@ -232,6 +238,7 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
     t.inv = upload(inv);
     t.qmod = upload(qmod);
     t.vq = upload(vq);
+    t.qmodd = upload(qmodd);
     return t;
 }
 

@@ -590,6 +590,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     uint8_t *vb = reinterpret_cast<uint8_t *>(dsm + 3 * kTile);
     Tw *tws = reinterpret_cast<Tw *>(dsm + 3 * kTile + kTile / 8); // the column table, staged
     __shared__ uint64_t tq[8], tv[9];
+    __shared__ double tqd[8][2];
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y / limbs, l = blockIdx.y % limbs;
     const int poly = pd / src.ndigits, d = pd % src.ndigits;
@@ -631,12 +632,20 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         for (int i = tid; i < 2 * S; i += kPhaseThreads) dst[i] = src[i];
     }
     if (mode == 2) {
+        const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
+        const int row = l < L1 ? l : src.nQ + (l - L1);
+        // float64 multSum when the digit's sources and this target are all
+        // below 2^50: each y_i * (Q/q_i mod p) reduced by mulmod_f (|.| <= 5p/8),
+        // the four terms and the correction summed and reduced to centered
+        const bool fpm = fp && tb->fp_src;
         if (tid < 2 * ns + 1) {
-            const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
-            const int row = l < L1 ? l : src.nQ + (l - L1);
-            if (tid < ns)
+            if (tid < ns) {
                 tq[tid] = tb->qmod[row * ns + tid];
-            else
+                if (fpm) {
+                    tqd[tid][0] = tb->qmodd[(row * ns + tid) * 2];
+                    tqd[tid][1] = tb->qmodd[(row * ns + tid) * 2 + 1];
+                }
+            } else
                 tv[tid - ns] = tb->vq[row * (ns + 1) + (tid - ns)];
         }
         const uint64_t *yp = src.y + (long long)pd * src.alpha * N + blockIdx.x * C;
@@ -657,28 +666,54 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         }
         issue(0, stg);
         issue(1, stg + kTile);
-        uint64_t lo[8], hi[8];
+        if (fpm) {
+            double acc[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) lo[e] = hi[e] = 0;
-        for (int i = 0; i < ns; ++i) {
-            if (i + 1 < ns)
-                cp_async_wait<1>();
-            else
-                cp_async_wait<0>();
-            __syncthreads();
-            const uint64_t *buf = stg + (i & 1) * kTile;
-            const uint64_t b = tq[i];
+            for (int e = 0; e < 8; ++e) acc[e] = 0.0;
+            for (int i = 0; i < ns; ++i) {
+                if (i + 1 < ns)
+                    cp_async_wait<1>();
+                else
+                    cp_async_wait<0>();
+                __syncthreads();
+                const uint64_t *buf = stg + (i & 1) * kTile;
+                const double cw = tqd[i][0], cq = tqd[i][1];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) mac128(lo[e], hi[e], buf[e * kPhaseThreads + tid], b);
-            __syncthreads();
-            if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
-        }
+                for (int e = 0; e < 8; ++e)
+                    acc[e] = __dadd_rn(acc[e], mulmod_f(u64_to_f(buf[e * kPhaseThreads + tid]), cw, cq, md.qd));
+                __syncthreads();
+                if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
+            }
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int idx = e * kPhaseThreads + tid;
-            const uint64_t h = __umul64hi(lo[e] * md.qinv, q);
-            const uint64_t r = canon3(hi[e] - h + q + tv[vb[idx]], q);
-            s[saddr<S>(idx % C, idx / C)] = fp ? (uint64_t)__double_as_longlong(centered_f(r, q)) : r;
+            for (int e = 0; e < 8; ++e) {
+                const int idx = e * kPhaseThreads + tid;
+                const double x = __dadd_rn(acc[e], u64_to_f(tv[vb[idx]]));
+                s[saddr<S>(idx % C, idx / C)] = (uint64_t)__double_as_longlong(reduce_f(x, md.qinvd, md.qd));
+            }
+        } else {
+            uint64_t lo[8], hi[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) lo[e] = hi[e] = 0;
+            for (int i = 0; i < ns; ++i) {
+                if (i + 1 < ns)
+                    cp_async_wait<1>();
+                else
+                    cp_async_wait<0>();
+                __syncthreads();
+                const uint64_t *buf = stg + (i & 1) * kTile;
+                const uint64_t b = tq[i];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) mac128(lo[e], hi[e], buf[e * kPhaseThreads + tid], b);
+                __syncthreads();
+                if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int idx = e * kPhaseThreads + tid;
+                const uint64_t h = __umul64hi(lo[e] * md.qinv, q);
+                const uint64_t r = canon3(hi[e] - h + q + tv[vb[idx]], q);
+                s[saddr<S>(idx % C, idx / C)] = fp ? (uint64_t)__double_as_longlong(centered_f(r, q)) : r;
+            }
         }
     } else {
         const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)(mode == 0 ? start : l) * N;
