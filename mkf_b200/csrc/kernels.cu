@@ -104,36 +104,62 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
 }
 
 // y_i and the float64 correction of every (poly, digit, coefficient)
+// (reconstructRNS, basis_extension.go:537-579), written column-major for the
+// digit column pass: coefficient r*2^n2 + cc goes to cc*2^n1 + r.  A block
+// reads a 32x32 tile of (r, cc) along cc and writes it along r through
+// shared memory.
 __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in, long long in_pstride,
                                                              const ModUpTab *tabs,
                                                              const DevModulus *mods, uint64_t *y,
                                                              uint8_t *v, int level, int alpha,
-                                                             int ndigits, int N) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= N) return;
+                                                             int ndigits, int N, int n1, int n2) {
+    __shared__ uint64_t tile[32][33];
+    __shared__ uint8_t vt[32][33];
     const int d = blockIdx.y, p = blockIdx.z;
     const int ns = (level > alpha * (d + 1) - 1 ? alpha - 2 : (level % alpha) - 1) + 2;
     if (ns < 2) return;
     const ModUpTab tab = tabs[d * (alpha + 1) + ns];
-    const uint64_t *xp = in + (long long)p * in_pstride + (long long)d * alpha * N + x;
+    const int ctiles = (1 << n2) / 32;
+    const int r0 = (blockIdx.x / ctiles) * 32, c0 = (blockIdx.x % ctiles) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const uint64_t *xp = in + (long long)p * in_pstride + (long long)d * alpha * N;
     const long long pd = (long long)p * ndigits + d;
-    uint64_t *yp = y + pd * alpha * N + x;
-    double vi = 0.0;
+    uint64_t *yp = y + pd * alpha * N;
+    double vi[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < ns; ++i) {
+        const DevModulus &m = mods[tab.src_mod[i]];
+        const uint64_t inv = tab.inv[i];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        if (i < ns) {
-            const DevModulus &m = mods[tab.src_mod[i]];
-            const uint64_t yi = mred(xp[(long long)i * N], tab.inv[i], m.q, m.qinv);
-            yp[(long long)i * N] = yi;
-            vi = __dadd_rn(vi, __ddiv_rn(__ull2double_rn(yi), m.qd));
+        for (int k = 0; k < 4; ++k) {
+            const int rr = ty + 8 * k;
+            const uint64_t yi = mred(xp[(long long)i * N + ((long long)(r0 + rr) << n2) + c0 + tx], inv, m.q, m.qinv);
+            vi[k] = __dadd_rn(vi[k], __ddiv_rn(__ull2double_rn(yi), m.qd));
+            tile[rr][tx] = yi;
         }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int cj = ty + 8 * k;
+            yp[(long long)i * N + ((long long)(c0 + cj) << n1) + r0 + tx] = tile[tx][cj];
+        }
+        __syncthreads();
     }
-    v[pd * N + x] = (uint8_t)__double2ull_rz(vi);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) vt[ty + 8 * k][tx] = (uint8_t)__double2ull_rz(vi[k]);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int cj = ty + 8 * k;
+        v[pd * N + ((long long)(c0 + cj) << n1) + r0 + tx] = vt[tx][cj];
+    }
 }
 
-size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys) {
+size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys, int level,
+                                   bool with_t) {
     const size_t n = (size_t)npolys * ndigits * c.N;
-    return n * c.alpha_of(gamma) + (n + 7) / 8 + 64;
+    size_t w = n * c.alpha_of(gamma) + (n + 7) / 8 + 64;
+    if (with_t && c.n2) w += (size_t)npolys * ndigits * (level + 1 + c.nP) * c.N;
+    return w;
 }
 
 void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
@@ -152,11 +178,13 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     const size_t n = (size_t)npolys * ndigits * c.N;
     uint64_t *y = scratch;
     uint8_t *v = reinterpret_cast<uint8_t *>(scratch + n * alpha);
+    uint64_t *tbuf = scratch + n * alpha + (n + 7) / 8 + 64;
     if (!ring_r && alpha >= 2) {
         ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
         note_launch();
-        digits_prep_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(
-            in, in_pstride, c.d_decomp[gamma - 1], c.d_mods, y, v, level, alpha, ndigits, c.N);
+        digits_prep_kernel<<<dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st>>>(
+            in, in_pstride, c.d_decomp[gamma - 1], c.d_mods, y, v, level, alpha, ndigits, c.N,
+            c.n1, c.n2);
     }
     DigitSrc src;
     src.x = in;
@@ -169,7 +197,7 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     src.level = level;
     src.nQ = c.nQ;
     if (own && !ring_r) src.own = *own;
-    ntt_forward_digits(c, src, out, npolys, st);
+    ntt_forward_digits(c, src, out, npolys, tbuf, st);
 }
 
 bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride, int level,
@@ -184,8 +212,9 @@ bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride
     if (alpha >= 2) {
         ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
         note_launch();
-        digits_prep_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(
-            in, in_pstride, c.d_decomp[0], c.d_mods, y, v, level, alpha, ndigits, c.N);
+        digits_prep_kernel<<<dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st>>>(
+            in, in_pstride, c.d_decomp[0], c.d_mods, y, v, level, alpha, ndigits, c.N, c.n1,
+            c.n2);
     }
     DigitSrc src;
     src.x = in;

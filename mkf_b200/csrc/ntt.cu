@@ -37,6 +37,9 @@ struct NttArgs {
     // row pass of gadget digits [poly][digit][limb]: skip each digit's own
     // limbs (already final, copied by the column pass); 0 = transform all
     int own_alpha = 0, own_ndigits = 0, own_level = 0;
+    // row pass: read the column pass's output from here, column-major, laid
+    // out like ls (null: in place, row-major)
+    const uint64_t *in_t = nullptr;
 };
 
 // Number of source limbs of digit d (decomposeAndSplit's p0idxed - p0idxst,
@@ -355,6 +358,19 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
     }
 }
 
+// Row-pass tile of C rows read from a column-major limb (row r, column cc at
+// cc*S1 + r): for each column the tile's C rows are contiguous.
+template <int LOGS>
+MKF_DEV void tile_load_t(uint64_t *s, const uint64_t *data, int S1, int tid) {
+    constexpr int S = 1 << LOGS, C = kTile / S;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const int idx = e * kPhaseThreads + tid;
+        const int cc = idx / C, rr = idx % C;
+        s[saddr<S>(rr, cc)] = data[(long long)cc * S1 + blockIdx.x * C + rr];
+    }
+}
+
 // Store reductions: none, [0,4q) -> [0,q), any -> [0,q), any -> [0,2q),
 // centered double -> [0,q).
 enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q, kRedF };
@@ -388,7 +404,8 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
 // The butterfly passes of a forward phase on the tile in shared memory.
 // KEEP: the last pass leaves its 8 words in vout (thread t of column c then
 // holds points 8t..8t+7 of its sub-transform) instead of storing them.
-template <int LOGS, bool LAZY, bool KEEP = false, bool TWS = false>
+// REGIN: the first pass takes its words (points elem(0, t, r)) from vout.
+template <int LOGS, bool LAZY, bool KEEP = false, bool TWS = false, bool REGIN = false>
 MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
                         uint64_t *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
@@ -397,7 +414,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[saddr<S>(c, elem<LOGS>(p, t, r))];
+        for (int r = 0; r < 8; ++r) v[r] = (REGIN && p == 0) ? vout[r] : s[saddr<S>(c, elem<LOGS>(p, t, r))];
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const int st = 3 * p + u;
@@ -430,7 +447,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
 // the bits of centered doubles, and every pass ends by reducing its words to
 // |x| <= q/2, so that the next pass (or phase) starts centered again.  KEEP:
 // the last pass leaves its words in vout, centered.
-template <int LOGS, bool KEEP = false, bool TWS = false>
+template <int LOGS, bool KEEP = false, bool TWS = false, bool REGIN = false>
 MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c, int t,
                           double *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
@@ -438,7 +455,9 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+        for (int r = 0; r < 8; ++r)
+            v[r] = (REGIN && p == 0) ? vout[r]
+                                     : __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const int st = 3 * p + u;
@@ -489,6 +508,8 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     const bool fp = q < kFp64Bound;
     if (COLS && fp)
         tile_load<LOGS, true, true>(s, data, R, tid, md.qinvd, md.qd);
+    else if (!COLS && a.in_t)
+        tile_load_t<LOGS>(s, a.in_t + (long long)poly * a.ls.poly_stride + (long long)l * N, 1 << a.n1, tid);
     else
         tile_load<LOGS, COLS>(s, data, R, tid);
     // the column pass stages its table (S entries, shared by every column) in
@@ -568,29 +589,24 @@ MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
         : "l"(a), "l"(b));
 }
 
-// Dynamic shared memory of the digit column pass: the NTT tile, two staging
-// tiles for y_i and one byte per word for the float64 correction.
-constexpr size_t kDigitsSmem = 3 * kTile * sizeof(uint64_t) + kTile + 256 * sizeof(Tw);
-
 // Column pass of the NTT of gadget digits with the decomposition fused into
-// the load: every word of the tile is reconstructed from the digit's y_i and
-// float64 correction v (multSum, basis_extension.go:581-646), copied from an
-// own limb, or copied raw from a one-limb digit, instead of being read back
-// from a stored digit polynomial.  Grid rows enumerate (poly, digit, limb).
-// The y_i tiles are streamed into shared memory with asynchronous copies,
-// two in flight, so that the multiply-accumulate never waits on single loads.
-// multSum's 128-bit sum needs no reduction on the way: its high word stays
-// below ns * q_i * p_j / 2^64 < p_j.
+// its first radix-8 pass.  Every column of a digit limb belongs to T = S/8
+// lanes of one warp, so the pass needs no block-wide barrier: a multSum word
+// (basis_extension.go:581-646) is rebuilt from the digit's y_i and float64
+// correction v, which the prep kernel stores column-major (coefficient
+// r*2^n2 + cc at cc*2^n1 + r), straight into the registers of the first
+// pass, and the transformed column is written column-major as well (the row
+// pass reads it so).  One-limb digits and own limbs without an NTT-domain
+// copy are reduced from the coefficient-domain input instead, through a
+// shared-memory tile.  Own limbs with an NTT-domain input are copied, in the
+// standard layout, to src.own_out.  Grid rows enumerate (poly, digit, limb).
+// The integer multSum's 128-bit sum needs no reduction on the way: its high
+// word stays below ns * q_i * p_j / 2^64 < p_j.
 template <int LOGS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    extern __shared__ __align__(16) uint64_t dsm[];
-    uint64_t *s = dsm;
-    uint64_t *stg = dsm + kTile;
-    uint8_t *vb = reinterpret_cast<uint8_t *>(dsm + 3 * kTile);
-    Tw *tws = reinterpret_cast<Tw *>(dsm + 3 * kTile + kTile / 8); // the column table, staged
-    __shared__ uint64_t tq[8], tv[9];
-    __shared__ double tqd[8][2];
+    __shared__ uint64_t s[kTile];
+    __shared__ __align__(16) uint64_t twsm[2 * S]; // the column table (Tw or TwD)
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y / limbs, l = blockIdx.y % limbs;
     const int poly = pd / src.ndigits, d = pd % src.ndigits;
@@ -613,7 +629,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
                                   ? src.own.p[0] + (long long)gp * src.own.pstride[0]
                                   : src.own.p[1] + (long long)(gp - src.own.split) * src.own.pstride[1]) +
                              (long long)l * N;
-        uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N;
+        uint64_t *dst = src.own_out + (long long)pd * a.ls.poly_stride + (long long)l * N;
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             const int idx = e * kPhaseThreads + tid;
@@ -626,115 +642,91 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     // doubles and leave it as doubles for the row pass
     const bool fp = q < kFp64Bound;
     {
-        const uint64_t *src = fp ? reinterpret_cast<const uint64_t *>(a.tw1d + (size_t)m * (1 << a.n1))
-                                 : reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * (1 << a.n1));
-        uint64_t *dst = reinterpret_cast<uint64_t *>(tws);
-        for (int i = tid; i < 2 * S; i += kPhaseThreads) dst[i] = src[i];
+        const uint64_t *tsrc = fp ? reinterpret_cast<const uint64_t *>(a.tw1d + (size_t)m * S)
+                                  : reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * S);
+        for (int i = tid; i < 2 * S; i += kPhaseThreads) twsm[i] = __ldg(tsrc + i);
     }
+    const int col = blockIdx.x * C + c;
+    // first-pass words (points r*T + t of column col): canonical words, or
+    // the bits of centered doubles for float64 limbs
+    uint64_t vi[8];
     if (mode == 2) {
         const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
         const int row = l < L1 ? l : src.nQ + (l - L1);
-        // float64 multSum when the digit's sources and this target are all
-        // below 2^50: each y_i * (Q/q_i mod p) reduced by mulmod_f (|.| <= 5p/8),
-        // the four terms and the correction summed and reduced to centered
-        const bool fpm = fp && tb->fp_src;
-        if (tid < 2 * ns + 1) {
-            if (tid < ns) {
-                tq[tid] = tb->qmod[row * ns + tid];
-                if (fpm) {
-                    tqd[tid][0] = tb->qmodd[(row * ns + tid) * 2];
-                    tqd[tid][1] = tb->qmodd[(row * ns + tid) * 2 + 1];
-                }
-            } else
-                tv[tid - ns] = tb->vq[row * (ns + 1) + (tid - ns)];
-        }
-        const uint64_t *yp = src.y + (long long)pd * src.alpha * N + blockIdx.x * C;
-        const uint8_t *vp = src.v + (long long)pd * N + blockIdx.x * C;
-        // tile word w = r*C + cc sits at coefficient r*R + cc of the column tile
-        auto issue = [&](int i, uint64_t *buf) {
-            const uint64_t *g = yp + (long long)i * N;
-#pragma unroll
-            for (int k = 0; k < kTile / 2 / kPhaseThreads; ++k) {
-                const int w = 2 * (k * kPhaseThreads + tid);
-                cp_async16(buf + w, g + (w / C) * R + w % C);
-            }
-            cp_async_commit();
-        };
-        if (tid < kTile / 16) {
-            const int b = 16 * tid;
-            cp_async16(vb + b, vp + (b / C) * R + b % C);
-        }
-        issue(0, stg);
-        issue(1, stg + kTile);
-        if (fpm) {
+        const uint64_t *yp = src.y + (long long)pd * src.alpha * N + (long long)col * S + t;
+        const uint8_t *vp = src.v + (long long)pd * N + (long long)col * S + t;
+        const uint64_t *tvr = tb->vq + row * (ns + 1);
+        if (fp && tb->fp_src) {
+            // float64 multSum: each y_i * (Q/q_i mod p) reduced by mulmod_f
+            // (|.| <= 5p/8), the terms and the correction summed, then centered
             double acc[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) acc[e] = 0.0;
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
             for (int i = 0; i < ns; ++i) {
-                if (i + 1 < ns)
-                    cp_async_wait<1>();
-                else
-                    cp_async_wait<0>();
-                __syncthreads();
-                const uint64_t *buf = stg + (i & 1) * kTile;
-                const double cw = tqd[i][0], cq = tqd[i][1];
+                const double cw = __ldg(tb->qmodd + (row * ns + i) * 2);
+                const double cq = __ldg(tb->qmodd + (row * ns + i) * 2 + 1);
+                const uint64_t *yi = yp + (long long)i * N;
 #pragma unroll
-                for (int e = 0; e < 8; ++e)
-                    acc[e] = __dadd_rn(acc[e], mulmod_f(u64_to_f(buf[e * kPhaseThreads + tid]), cw, cq, md.qd));
-                __syncthreads();
-                if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
+                for (int r = 0; r < 8; ++r)
+                    acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(__ldg(yi + r * T)), cw, cq, md.qd));
             }
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int idx = e * kPhaseThreads + tid;
-                const double x = __dadd_rn(acc[e], u64_to_f(tv[vb[idx]]));
-                s[saddr<S>(idx % C, idx / C)] = (uint64_t)__double_as_longlong(reduce_f(x, md.qinvd, md.qd));
-            }
+            for (int r = 0; r < 8; ++r)
+                vi[r] = (uint64_t)__double_as_longlong(
+                    reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + __ldg(vp + r * T)))), md.qinvd, md.qd));
         } else {
-            uint64_t lo[8], hi[8];
+            // integer multSum, four words at a time
 #pragma unroll
-            for (int e = 0; e < 8; ++e) lo[e] = hi[e] = 0;
-            for (int i = 0; i < ns; ++i) {
-                if (i + 1 < ns)
-                    cp_async_wait<1>();
-                else
-                    cp_async_wait<0>();
-                __syncthreads();
-                const uint64_t *buf = stg + (i & 1) * kTile;
-                const uint64_t b = tq[i];
+            for (int h = 0; h < 8; h += 4) {
+                uint64_t lo[4], hi[4];
 #pragma unroll
-                for (int e = 0; e < 8; ++e) mac128(lo[e], hi[e], buf[e * kPhaseThreads + tid], b);
-                __syncthreads();
-                if (i + 2 < ns) issue(i + 2, stg + (i & 1) * kTile);
-            }
+                for (int r = 0; r < 4; ++r) lo[r] = hi[r] = 0;
+                for (int i = 0; i < ns; ++i) {
+                    const uint64_t b = __ldg(tb->qmod + row * ns + i);
+                    const uint64_t *yi = yp + (long long)i * N + h * T;
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int idx = e * kPhaseThreads + tid;
-                const uint64_t h = __umul64hi(lo[e] * md.qinv, q);
-                const uint64_t r = canon3(hi[e] - h + q + tv[vb[idx]], q);
-                s[saddr<S>(idx % C, idx / C)] = fp ? (uint64_t)__double_as_longlong(centered_f(r, q)) : r;
+                    for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], __ldg(yi + r * T), b);
+                }
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
+                    const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + __ldg(vp + (h + r) * T)), q);
+                    vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+                }
             }
         }
     } else {
+        // coefficient-domain source limb, transposed through the tile
         const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)(mode == 0 ? start : l) * N;
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             const int idx = e * kPhaseThreads + tid;
             const int r = idx / C, cc = idx % C;
-            const uint64_t x = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
-            s[saddr<S>(cc, r)] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+            s[saddr<S>(cc, r)] = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t x = s[saddr<S>(c, elem<LOGS>(0, t, r))];
+            vi[r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
         }
     }
-    __syncthreads();
-    if (fp)
-        fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
-    else if (q < kLazyBound)
-        fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
-    else
-        fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
-    __syncthreads();
-    uint64_t *data = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N;
-    tile_store<LOGS, true>(s, data, R, tid, md, kRedNone);
+    __syncthreads(); // the staged table
+    uint64_t *out = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + (long long)col * S + 8 * t;
+    if (fp) {
+        double vf[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)vi[r]);
+        fwd_passes_f<LOGS, true, true, true>(s, reinterpret_cast<const TwD *>(twsm), md.qd, md.qinvd, c, t, vf);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) vi[r] = (uint64_t)__double_as_longlong(vf[r]);
+    } else if (q < kLazyBound) {
+        fwd_passes<LOGS, true, true, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
+    } else {
+        fwd_passes<LOGS, false, true, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r += 2) *reinterpret_cast<ulonglong2 *>(out + r) = make_ulonglong2(vi[r], vi[r + 1]);
 }
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
@@ -872,18 +864,6 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
     }
 }
 
-// Opt a digit column kernel into kDigitsSmem bytes of dynamic shared memory,
-// once per kernel and device.
-template <typename K> static void digits_smem_attr(K kernel, int device) {
-    static std::mutex mu;
-    static std::set<std::pair<const void *, int>> done;
-    std::lock_guard<std::mutex> g(mu);
-    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), device);
-    if (done.count(key)) return;
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDigitsSmem);
-    done.insert(key);
-}
-
 // Dynamic shared memory of the fused row pass: the NTT tile and two
 // accumulator tiles.
 constexpr size_t kRowIpSmem = 3 * kTile * sizeof(uint64_t);
@@ -908,7 +888,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const DevModulus md = a.mods[m];
     const uint64_t q = md.q;
     const bool lazy = q < kLazyBound;
-    const int N = 1 << a.logN, R = 1 << a.n2;
+    const int N = 1 << a.logN;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
     const long long base = (long long)blockIdx.x * kTile + c * S + 8 * t;
     uint64_t *acc0 = dsm + kTile + c * S + 8 * t;
@@ -939,7 +919,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
         } else {
             const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N;
             __syncthreads(); // the previous digit's tile is consumed
-            tile_load<LOGS, false>(s, src, R, tid);
+            tile_load_t<LOGS>(s, src, 1 << a.n1, tid);
             __syncthreads();
             if (fp) {
                 // centered doubles -> [0,q) words (MRed takes any 64-bit word)
@@ -1023,10 +1003,10 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             sb.y = src.y + (long long)p0 * src.alpha * c.N;                                        \
             sb.v = src.v + (long long)p0 * c.N;                                                    \
             sb.poly0 = first_poly;                                                                 \
+            sb.own_out = b.ls.base;                                                                \
             dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs);                                     \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
-            smem_attr(ntt_fwd_digits_col<L1G>, c.device, kDigitsSmem);                             \
-            ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
+            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(b, sb);                                  \
             if (p0) note_launch(1);                                                                \
         }                                                                                          \
         dim3 g2((1 << L1G) / (kTile >> L2G), limbs, ip.groups * ip.nin);                           \
@@ -1053,13 +1033,10 @@ void ntt_prepare(const Context &c) {
     smem_attr(ntt_fwd_phase<8, false>, c.device, fwd_phase_smem<8, false>());
     smem_attr(ntt_digits_row_ip<7>, c.device, kRowIpSmem);
     smem_attr(ntt_digits_row_ip<8>, c.device, kRowIpSmem);
-    digits_smem_attr(ntt_fwd_digits_col<6>, c.device);
-    digits_smem_attr(ntt_fwd_digits_col<7>, c.device);
-    digits_smem_attr(ntt_fwd_digits_col<8>, c.device);
 }
 
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
-                        cudaStream_t st) {
+                        uint64_t *tbuf, cudaStream_t st) {
     const int L1 = src.level + 1, limbs = L1 + c.nP;
     const int np = npolys * src.ndigits;
     if (np <= 0) return;
@@ -1077,14 +1054,18 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
     const int max_polys = std::max(src.ndigits, (65535 / limbs) / src.ndigits * src.ndigits);
     for (int p0 = 0; p0 < np; p0 += max_polys) {
         const int npp = std::min(max_polys, np - p0);
-        NttArgs b = a;
+        // column pass: tbuf (column-major); row pass: tbuf -> out
+        NttArgs b = a, bt = a;
         b.ls.base = out + (long long)p0 * a.ls.poly_stride;
+        b.in_t = tbuf + (long long)p0 * a.ls.poly_stride;
+        bt.ls.base = tbuf + (long long)p0 * a.ls.poly_stride;
         DigitSrc sb = src;
         const int first_poly = p0 / src.ndigits;
         sb.x = src.x + (long long)first_poly * src.x_pstride;
         sb.y = src.y + (long long)p0 * src.alpha * c.N;
         sb.v = src.v + (long long)p0 * c.N;
         sb.poly0 = first_poly;
+        sb.own_out = b.ls.base;
         if (src.own.p[0]) {
             b.own_alpha = src.alpha;
             b.own_ndigits = src.ndigits;
@@ -1105,8 +1086,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
-            digits_smem_attr(ntt_fwd_digits_col<L1G>, c.device);                                   \
-            ntt_fwd_digits_col<L1G><<<g1, block, kDigitsSmem, st>>>(b, sb);                        \
+            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(bt, sb);                                 \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \

@@ -26,13 +26,17 @@ struct OwnNtt {
 struct DigitSrc {
     const uint64_t *x = nullptr;   // coefficient-domain source polynomials (ring limbs)
     long long x_pstride = 0;
-    const uint64_t *y = nullptr;   // [poly][digit][alpha][N]: y_i = MRed(x_i, (Q/q_i)^-1)
-    const uint8_t *v = nullptr;    // [poly][digit][N]: float64 correction
+    // y_i = MRed(x_i, (Q/q_i)^-1) at [poly][digit][alpha][N] and the float64
+    // correction at [poly][digit][N], each limb column-major (coefficient
+    // r*2^n2 + cc at cc*2^n1 + r)
+    const uint64_t *y = nullptr;
+    const uint8_t *v = nullptr;
     const ModUpTab *tabs = nullptr; // [digit][alpha+1] (null when every digit is one limb)
     int ndigits = 0, alpha = 0, level = 0, nQ = 0;
     OwnNtt own;    // optional
     int poly0 = 0; // index of the first polynomial of this launch in `own`
     int own_skip = 0; // own limbs are neither copied nor transformed
+    uint64_t *own_out = nullptr; // where own limbs are copied (set by the launchers)
 };
 
 // Inner product fused into the digits' row pass (ntt_forward_digits_ip):
@@ -54,12 +58,14 @@ struct DigitIpArgs {
     long long out_gstride = 0, out_istride = 0, out_ostride = 0;
 };
 // Column pass of the digits (as ntt_forward_digits) then the fused row pass
-// + inner product; logN 13..16.  dig receives the column-pass output.
+// + inner product; logN 13..16.  dig receives the column-pass output
+// (column-major limbs).
 void ntt_forward_digits_ip(const Context &c, const DigitSrc &src, uint64_t *dig, int npolys,
                            const DigitIpArgs &ip, cudaStream_t st);
-// NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load.
+// NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load;
+// tbuf (as large as out) holds the column pass's column-major output.
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
-                        cudaStream_t st);
+                        uint64_t *tbuf, cudaStream_t st);
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
 // Sets the kernels' launch attributes for c's device (idempotent); called
 // before a stream capture so that nothing but launches happens inside it.
