@@ -326,6 +326,10 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         }
         d.last = h_mulmod(irev[1], d.ninv, qq);
         d.last_sh = h_shoup(d.last, qq);
+        d.ninvd = (double)d.ninv;
+        d.ninvq = (double)d.ninv / (double)qq;
+        d.lastd = (double)d.last;
+        d.lastq = (double)d.last / (double)qq;
         for (int k = 0; k < S1; ++k) {
             fwd1[(size_t)m * S1 + k] = Tw{rev[k], h_shoup(rev[k], qq)};
             inv1[(size_t)m * S1 + k] = Tw{irev[k], h_shoup(irev[k], qq)};

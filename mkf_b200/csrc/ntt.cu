@@ -100,6 +100,16 @@ __device__ __forceinline__ void ct_bfly_f(double &U, double &V, const TwD w, dou
     V = __dadd_rn(u, -t);
 }
 
+// Float64 Gentleman-Sande butterfly: U' = U + V reduced to |U'| <= q/2 and
+// V' = (U - V) w.  From |U|, |V| <= B q with B <= 1 (|U - V| < 2q, the
+// rounding trick's range) V' stays below (1/2 + B/4) q, so the bound settles
+// near 2q/3 and every stage keeps it.
+__device__ __forceinline__ void gs_bfly_f(double &U, double &V, const TwD w, double q, double qi) {
+    const double x = reduce_f(__dadd_rn(U, V), qi, q);
+    V = mulmod_f(__dadd_rn(U, -V), w.w, w.wq, q);
+    U = x;
+}
+
 // MODE 0: whole limb in one tile. MODE 1: column pass. MODE 2: row pass.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) ntt_fwd_kernel(NttArgs a) {
@@ -333,9 +343,9 @@ MKF_DEV TwD ldtwd_s(const TwD *p) {
     return TwD{v.x, v.y};
 }
 
-// CONV: the words are integers below 2^52 that enter the float64 transform;
-// they are stored as the bits of their centered doubles.
-template <int LOGS, bool COLS, bool CONV = false>
+// CONV: the words enter the float64 transform and are stored as the bits of
+// their centered doubles; 1: any word below 2^52, 2: canonical words.
+template <int LOGS, bool COLS, int CONV = 0>
 MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double qi = 0.0,
                        double qd = 0.0) {
     constexpr int S = 1 << LOGS, C = kTile / S;
@@ -353,7 +363,8 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
             a = saddr<S>(cc, j);
             v = data[(long long)blockIdx.x * kTile + idx];
         }
-        if (CONV) v = (uint64_t)__double_as_longlong(reduce_f(u64_to_f(v), qi, qd));
+        if (CONV == 1) v = (uint64_t)__double_as_longlong(reduce_f(u64_to_f(v), qi, qd));
+        if (CONV == 2) v = (uint64_t)__double_as_longlong(centered_f(v, (uint64_t)qd));
         s[a] = v;
     }
 }
@@ -506,8 +517,57 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     // float64 limbs: the column pass converts the input words, the row pass
     // reads the column pass's doubles and stores canonical words
     const bool fp = q < kFp64Bound;
+    if (!COLS) {
+        // row phase: each row belongs to T lanes of one warp.  Its words are
+        // loaded straight into the first radix-8 pass (a row-major input) or
+        // staged through the tile (a column-major one), and the last pass
+        // stores its consecutive points from registers.
+        const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+        uint64_t v[8];
+        if (a.in_t) {
+            tile_load_t<LOGS>(s, a.in_t + (long long)poly * a.ls.poly_stride + (long long)l * N, 1 << a.n1, tid);
+            __syncthreads();
+        } else {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = data[rowoff + r * T + t];
+        }
+        // the last pass leaves the row in the warp's tile region; it is
+        // stored from there in point order (lane t: points k*T + t)
+        if (fp) {
+            double vf[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
+            const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            if (a.in_t)
+                fwd_passes_f<LOGS>(s, twd, md.qd, md.qinvd, c, t);
+            else
+                fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
+        } else {
+            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            if (lazy) {
+                if (a.in_t)
+                    fwd_passes<LOGS, true>(s, tw, q, c, t);
+                else
+                    fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    data[rowoff + k * T + t] = reduce_any(s[saddr<S>(c, k * T + t)], q, md.one_sh);
+            } else {
+                if (a.in_t)
+                    fwd_passes<LOGS, false>(s, tw, q, c, t);
+                else
+                    fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[saddr<S>(c, k * T + t)], q);
+            }
+        }
+        return;
+    }
     if (COLS && fp)
-        tile_load<LOGS, true, true>(s, data, R, tid, md.qinvd, md.qd);
+        tile_load<LOGS, true, 1>(s, data, R, tid, md.qinvd, md.qd);
     else if (!COLS && a.in_t)
         tile_load_t<LOGS>(s, a.in_t + (long long)poly * a.ls.poly_stride + (long long)l * N, 1 << a.n1, tid);
     else
@@ -712,21 +772,20 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
         }
     }
     __syncthreads(); // the staged table
-    uint64_t *out = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + (long long)col * S + 8 * t;
     if (fp) {
         double vf[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)vi[r]);
-        fwd_passes_f<LOGS, true, true, true>(s, reinterpret_cast<const TwD *>(twsm), md.qd, md.qinvd, c, t, vf);
-#pragma unroll
-        for (int r = 0; r < 8; ++r) vi[r] = (uint64_t)__double_as_longlong(vf[r]);
+        fwd_passes_f<LOGS, false, true, true>(s, reinterpret_cast<const TwD *>(twsm), md.qd, md.qinvd, c, t, vf);
     } else if (q < kLazyBound) {
-        fwd_passes<LOGS, true, true, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
+        fwd_passes<LOGS, true, false, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
     } else {
-        fwd_passes<LOGS, false, true, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
+        fwd_passes<LOGS, false, false, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
     }
+    // the column leaves the warp's tile region in point order (lane t: points k*T + t)
+    uint64_t *out = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + (long long)col * S + t;
 #pragma unroll
-    for (int r = 0; r < 8; r += 2) *reinterpret_cast<ulonglong2 *>(out + r) = make_ulonglong2(vi[r], vi[r + 1]);
+    for (int k = 0; k < 8; ++k) out[k * T] = s[saddr<S>(c, k * T + t)];
 }
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
@@ -773,6 +832,44 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
     }
 }
 
+// The passes of an inverse phase in float64 (limbs below 2^50), on the bits
+// of centered doubles; COLS: the last phase, whose global stage 0 folds in
+// N^-1 (both outputs then below 2q/3).
+template <int LOGS, bool COLS>
+MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int c, int t) {
+    constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    const double q = md.qd, qi = md.qinvd;
+    double v[8];
+#pragma unroll
+    for (int p = NP - 1; p >= 0; --p) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+#pragma unroll
+        for (int u = 2; u >= 0; --u) {
+            const int st = 3 * p + u;
+            if (st < LOGS) {
+                const int stride = 1 << (LOGS - 1 - st - pass_pos<LOGS>(p));
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    if (r & stride) continue;
+                    double &U = v[r], &V = v[r + stride];
+                    if (COLS && st == 0) {
+                        const double x = mulmod_f(__dadd_rn(U, V), md.ninvd, md.ninvq, q);
+                        V = mulmod_f(__dadd_rn(U, -V), md.lastd, md.lastq, q);
+                        U = x;
+                    } else {
+                        const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
+                        gs_bfly_f(U, V, ldtwd(tw + (1 << st) + i), q, qi);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = (uint64_t)__double_as_longlong(v[r]);
+        __syncwarp();
+    }
+}
+
 template <int LOGS, bool COLS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
@@ -786,6 +883,53 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    if (!COLS) {
+        // row phase: each row belongs to T lanes of one warp, loaded into and
+        // stored from the warp's tile region in point order (lane t: points
+        // k*T + t); no block-wide barrier
+        const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+        const bool fp = md.q < kFp64Bound;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t x = data[rowoff + k * T + t];
+            s[saddr<S>(c, k * T + t)] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
+        }
+        __syncwarp();
+        if (fp) {
+            inv_passes_f<LOGS, false>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md, c, t);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[saddr<S>(c, k * T + t)];
+        } else {
+            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            if (lazy) {
+                inv_passes<LOGS, false, true>(s, tw, md, c, t);
+                // the first phase hands the second one values below 2q
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    data[rowoff + k * T + t] = reduce_2q(s[saddr<S>(c, k * T + t)], md.q, md.one_sh);
+            } else {
+                inv_passes<LOGS, false, false>(s, tw, md, c, t);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[saddr<S>(c, k * T + t)];
+            }
+        }
+        return;
+    }
+    if (md.q < kFp64Bound) {
+        // float64 limbs: the row phase converts the canonical input, the
+        // column phase reads its doubles and stores canonical words
+        if (COLS)
+            tile_load<LOGS, true>(s, data, R, tid);
+        else
+            tile_load<LOGS, false, 2>(s, data, R, tid, md.qinvd, md.qd);
+        __syncthreads();
+        const TwD *tw = COLS ? a.tw1d + (size_t)m * (1 << a.n1)
+                             : a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+        inv_passes_f<LOGS, COLS>(s, tw, md, c, t);
+        __syncthreads();
+        tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedF : kRedNone);
+        return;
+    }
     tile_load<LOGS, COLS>(s, data, R, tid);
     __syncthreads();
     const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
