@@ -123,7 +123,7 @@ static FoldScratch take_fold_scratch(const Context &c, Arena &ar, bool bfv, int 
     f.dig = ar.take(nops * kk * beta * qp);
     f.acc = ar.take(2 * nops * kk * qp);
     f.tmp = ar.take(2 * nops * poly);
-    f.dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, nops * k, level));
+    f.dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, nops * k));
     return f;
 }
 
@@ -279,7 +279,7 @@ std::string kklss_galois(const Context &c, Arena &ar, cudaStream_t st, int k, in
     uint64_t *H = ar.take(kk * beta * qp);
     uint64_t *E = ar.take(2 * kk * qp);
     uint64_t *tmp = ar.take(2 * kk * poly);
-    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, beta, k, level));
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, beta, k));
     if (ar.dry) return "";
     const uint64_t *src = in.data;
     long long scs = in.cs;
@@ -543,7 +543,7 @@ std::string kklss_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int sch
     uint64_t *ym = bfv ? ar.take(K1 * (long long)c.nQM * N) : nullptr;
     uint64_t *trs = bfv ? nullptr : ar.take(K1 * poly);
     uint8_t *ones = reinterpret_cast<uint8_t *>(ar.take(kMaxParties / 8 + 1));
-    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, nd, k, level));
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 2, nd, k));
     if (ar.dry) return "";
     fill_ones(ones, k, st);
 
@@ -718,7 +718,7 @@ std::string switch_one(const Context &c, Arena &ar, cudaStream_t st, int level, 
     uint64_t *dig = ar.take(beta * qp);
     uint64_t *acc = ar.take(2 * qp);
     uint64_t *tmp = ar.take(2 * poly);
-    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, 1, level));
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, 1, beta, 1));
     if (ar.dry) return "";
     d2d2(coeff, poly, in, poly, poly, 1, st);
     if (in_ntt) ntt_inverse(c, lsq(coeff, poly, L1), 1, st);
@@ -780,7 +780,7 @@ std::string decompose_poly(const Context &c, Arena &ar, cudaStream_t st, int gam
     if (c.nP % gamma) return "gamma must divide the number of special primes";
     if (c.nP / gamma > 8) return "at most 8 limbs per digit are supported";
     const int beta = c.beta_of(level, gamma);
-    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, gamma, beta, 1, level));
+    uint64_t *dscr = ar.take(decompose_ntt_scratch_words(c, gamma, beta, 1));
     if (ar.dry) return "";
     decompose_ntt(c, in_coeff, 0, 0, level, gamma, beta, out, 1, dscr, st);
     return "";

@@ -154,12 +154,9 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
     }
 }
 
-size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys, int level,
-                                   bool with_t) {
+size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys) {
     const size_t n = (size_t)npolys * ndigits * c.N;
-    size_t w = n * c.alpha_of(gamma) + (n + 7) / 8 + 64;
-    if (with_t && c.n2) w += (size_t)npolys * ndigits * (level + 1 + c.nP) * c.N;
-    return w;
+    return n * c.alpha_of(gamma) + (n + 7) / 8 + 64;
 }
 
 void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
@@ -178,7 +175,6 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     const size_t n = (size_t)npolys * ndigits * c.N;
     uint64_t *y = scratch;
     uint8_t *v = reinterpret_cast<uint8_t *>(scratch + n * alpha);
-    uint64_t *tbuf = scratch + n * alpha + (n + 7) / 8 + 64;
     if (!ring_r && alpha >= 2) {
         ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
         note_launch();
@@ -197,7 +193,7 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     src.level = level;
     src.nQ = c.nQ;
     if (own && !ring_r) src.own = *own;
-    ntt_forward_digits(c, src, out, npolys, tbuf, st);
+    ntt_forward_digits(c, src, out, npolys, st);
 }
 
 bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride, int level,

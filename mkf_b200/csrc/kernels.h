@@ -31,11 +31,8 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
 // the coefficient domain: a pre-pass writes y_i and the float64 correction
 // and the NTT column pass reconstructs each limb on load.  scratch must hold
 // decompose_ntt_scratch_words() words.  `own` (optional) gives the inputs in
-// the NTT domain: each digit's own limbs are copied from there.  with_t adds
-// the column pass's column-major intermediate (needed by decompose_ntt, not
-// by decompose_ntt_ip, which keeps it in dig).
-size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys, int level,
-                                   bool with_t = true);
+// the NTT domain: each digit's own limbs are copied from there.
+size_t decompose_ntt_scratch_words(const Context &c, int gamma, int ndigits, int npolys);
 void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, int ring_r,
                    int level, int gamma, int ndigits, uint64_t *out, int npolys,
                    uint64_t *scratch, cudaStream_t st, const OwnNtt *own = nullptr);

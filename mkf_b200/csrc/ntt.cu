@@ -37,9 +37,6 @@ struct NttArgs {
     // row pass of gadget digits [poly][digit][limb]: skip each digit's own
     // limbs (already final, copied by the column pass); 0 = transform all
     int own_alpha = 0, own_ndigits = 0, own_level = 0;
-    // row pass: read the column pass's output from here, column-major, laid
-    // out like ls (null: in place, row-major)
-    const uint64_t *in_t = nullptr;
 };
 
 // Number of source limbs of digit d (decomposeAndSplit's p0idxed - p0idxst,
@@ -369,19 +366,6 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
     }
 }
 
-// Row-pass tile of C rows read from a column-major limb (row r, column cc at
-// cc*S1 + r): for each column the tile's C rows are contiguous.
-template <int LOGS>
-MKF_DEV void tile_load_t(uint64_t *s, const uint64_t *data, int S1, int tid) {
-    constexpr int S = 1 << LOGS, C = kTile / S;
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        const int idx = e * kPhaseThreads + tid;
-        const int cc = idx / C, rr = idx % C;
-        s[saddr<S>(rr, cc)] = data[(long long)cc * S1 + blockIdx.x * C + rr];
-    }
-}
-
 // Store reductions: none, [0,4q) -> [0,q), any -> [0,q), any -> [0,2q),
 // centered double -> [0,q).
 enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q, kRedF };
@@ -518,19 +502,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     // reads the column pass's doubles and stores canonical words
     const bool fp = q < kFp64Bound;
     if (!COLS) {
-        // row phase: each row belongs to T lanes of one warp.  Its words are
-        // loaded straight into the first radix-8 pass (a row-major input) or
-        // staged through the tile (a column-major one), and the last pass
-        // stores its consecutive points from registers.
+        // row phase: each row belongs to T lanes of one warp; its words are
+        // loaded straight into the first radix-8 pass, and no block-wide
+        // barrier is needed.
         const long long rowoff = (long long)(blockIdx.x * C + c) * S;
         uint64_t v[8];
-        if (a.in_t) {
-            tile_load_t<LOGS>(s, a.in_t + (long long)poly * a.ls.poly_stride + (long long)l * N, 1 << a.n1, tid);
-            __syncthreads();
-        } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = data[rowoff + r * T + t];
-        }
+        for (int r = 0; r < 8; ++r) v[r] = data[rowoff + r * T + t];
         // the last pass leaves the row in the warp's tile region; it is
         // stored from there in point order (lane t: points k*T + t)
         if (fp) {
@@ -538,46 +516,34 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
             const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-            if (a.in_t)
-                fwd_passes_f<LOGS>(s, twd, md.qd, md.qinvd, c, t);
-            else
-                fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+            fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
             for (int k = 0; k < 8; ++k)
                 data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
-                if (a.in_t)
-                    fwd_passes<LOGS, true>(s, tw, q, c, t);
-                else
-                    fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
                     data[rowoff + k * T + t] = reduce_any(s[saddr<S>(c, k * T + t)], q, md.one_sh);
             } else {
-                if (a.in_t)
-                    fwd_passes<LOGS, false>(s, tw, q, c, t);
-                else
-                    fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[saddr<S>(c, k * T + t)], q);
             }
         }
         return;
     }
-    if (COLS && fp)
+    if (fp)
         tile_load<LOGS, true, 1>(s, data, R, tid, md.qinvd, md.qd);
-    else if (!COLS && a.in_t)
-        tile_load_t<LOGS>(s, a.in_t + (long long)poly * a.ls.poly_stride + (long long)l * N, 1 << a.n1, tid);
     else
-        tile_load<LOGS, COLS>(s, data, R, tid);
+        tile_load<LOGS, true>(s, data, R, tid);
     // the column pass stages its table (S entries, shared by every column) in
-    // shared memory; the row pass reads its per-row tables from global memory
-    // (staging the tile's C*S row twiddles measured slower)
+    // shared memory
     extern __shared__ __align__(16) uint64_t twdyn[];
     Tw *tws = reinterpret_cast<Tw *>(twdyn);
-    if (COLS) {
+    {
         const ulonglong2 *twg =
             fp ? reinterpret_cast<const ulonglong2 *>(a.tw1d + (size_t)m * (1 << a.n1))
                : reinterpret_cast<const ulonglong2 *>(a.tw1 + (size_t)m * (1 << a.n1));
@@ -585,30 +551,14 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         for (int i = tid; i < S; i += kPhaseThreads) d[i] = __ldg(twg + i);
     }
     __syncthreads();
-    if (fp) {
-        if (COLS)
-            fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
-        else
-            fwd_passes_f<LOGS>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md.qd,
-                               md.qinvd, c, t);
-        __syncthreads();
-        tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedNone : kRedF);
-        return;
-    }
-    if (COLS) {
-        if (lazy)
-            fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
-        else
-            fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
-    } else {
-        const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-        if (lazy)
-            fwd_passes<LOGS, true>(s, tw, q, c, t);
-        else
-            fwd_passes<LOGS, false>(s, tw, q, c, t);
-    }
+    if (fp)
+        fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
+    else if (lazy)
+        fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
+    else
+        fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
     __syncthreads();
-    tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedNone : lazy ? kRedAny : kRed4);
+    tile_store<LOGS, true>(s, data, R, tid, md, kRedNone);
 }
 
 // Dynamic shared memory of ntt_fwd_phase: its staged twiddles.
@@ -655,8 +605,8 @@ MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
 // (basis_extension.go:581-646) is rebuilt from the digit's y_i and float64
 // correction v, which the prep kernel stores column-major (coefficient
 // r*2^n2 + cc at cc*2^n1 + r), straight into the registers of the first
-// pass, and the transformed column is written column-major as well (the row
-// pass reads it so).  One-limb digits and own limbs without an NTT-domain
+// pass; the block's transformed columns are stored row-major through the
+// tile, for the row pass.  One-limb digits and own limbs without an NTT-domain
 // copy are reduced from the coefficient-domain input instead, through a
 // shared-memory tile.  Own limbs with an NTT-domain input are copied, in the
 // standard layout, to src.own_out.  Grid rows enumerate (poly, digit, limb).
@@ -782,10 +732,10 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a
     } else {
         fwd_passes<LOGS, false, false, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
     }
-    // the column leaves the warp's tile region in point order (lane t: points k*T + t)
-    uint64_t *out = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + (long long)col * S + t;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) out[k * T] = s[saddr<S>(c, k * T + t)];
+    // the tile holds every column of the block: store it row-major
+    __syncthreads();
+    tile_store<LOGS, true>(s, a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N, R, tid, md,
+                           kRedNone);
 }
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
@@ -1013,13 +963,14 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
 constexpr size_t kRowIpSmem = 3 * kTile * sizeof(uint64_t);
 
 // Row pass of the gadget digits fused with the key-switch inner product
-// (KeyswitchHoistedNoModDown, common.go:79-107): for one limb tile of one
-// polynomial (group g, input s), every digit is transformed in turn and its
-// words, still in registers after the last radix-8 pass, are multiplied by
-// the digit's two key polynomials and accumulated.  A digit's own limbs are
-// read from the NTT-domain input instead.  MRed(v, key) = v*key*2^-64 mod q
-// is canonical for any 64-bit v, so the lazy NTT outputs need no reduction,
-// and the sum equals the stand-alone inner product's exactly.
+// (KeyswitchHoistedNoModDown, common.go:79-107): for one row of one limb of
+// one polynomial (group g, input s), every digit is transformed in turn by
+// the warp that owns the row and its words are multiplied by the digit's two
+// key polynomials and accumulated, in the warp's region of two accumulator
+// tiles (no block-wide barrier).  A digit's own limbs are read from the
+// NTT-domain input instead.  MRed(v, key) = v*key*2^-64 mod q is canonical
+// for any 64-bit v, so the lazy integer outputs need no reduction, and the
+// sum equals the stand-alone inner product's exactly.
 template <int LOGS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a, DigitIpArgs g) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
@@ -1032,18 +983,19 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const DevModulus md = a.mods[m];
     const uint64_t q = md.q;
     const bool lazy = q < kLazyBound;
+    const bool fp = q < kFp64Bound;
     const int N = 1 << a.logN;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
-    const long long base = (long long)blockIdx.x * kTile + c * S + 8 * t;
-    uint64_t *acc0 = dsm + kTile + c * S + 8 * t;
+    const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+    // accumulators of this row, point order (lane t: points k*T + t)
+    uint64_t *acc0 = dsm + kTile + c * S + t;
     uint64_t *acc1 = acc0 + kTile;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) acc0[r] = acc1[r] = 0;
+    for (int k = 0; k < 8; ++k) acc0[k * T] = acc1[k * T] = 0;
     const uint64_t *kb = g.kptr[grp] ? g.kptr[grp] : g.B + (long long)grp * g.k_gstride;
-    const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N;
+    const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N + rowoff + t;
     const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
     const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-    const bool fp = q < kFp64Bound;
     for (int d = 0; d < g.beta; ++d) {
         const int start = d * g.alpha;
         const bool own = g.own.p[0] && l < g.L1 && l >= start &&
@@ -1053,48 +1005,46 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
             const uint64_t *xn = (poly < g.own.split
                                       ? g.own.p[0] + (long long)poly * g.own.pstride[0]
                                       : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
-                                 (long long)l * N + base;
+                                 (long long)l * N + rowoff + t;
 #pragma unroll
-            for (int r = 0; r < 8; r += 2) {
-                const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(xn + r);
-                v[r] = w.x;
-                v[r + 1] = w.y;
-            }
+            for (int k = 0; k < 8; ++k) v[k] = xn[k * T];
         } else {
-            const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N;
-            __syncthreads(); // the previous digit's tile is consumed
-            tile_load_t<LOGS>(s, src, 1 << a.n1, tid);
-            __syncthreads();
-            if (fp) {
-                // centered doubles -> [0,q) words (MRed takes any 64-bit word)
-                double vf[8];
-                fwd_passes_f<LOGS, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+            // the first radix-8 pass holds points r*T + t: load them directly
+            const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N + rowoff + t;
 #pragma unroll
-                for (int r = 0; r < 8; ++r) v[r] = canon_f(vf[r], md.qd);
-            } else if (lazy)
-                fwd_passes<LOGS, true, true>(s, tw, q, c, t, v);
-            else
-                fwd_passes<LOGS, false, true>(s, tw, q, c, t, v);
+            for (int r = 0; r < 8; ++r) v[r] = src[r * T];
+            if (fp) {
+                double vf[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
+                fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    v[k] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
+            } else {
+                if (lazy)
+                    fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
+                else
+                    fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = s[saddr<S>(c, k * T + t)];
+            }
         }
-        const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow + base;
+        const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
         const uint64_t *k1 = k0 + g.k_ostride;
 #pragma unroll
-        for (int r = 0; r < 8; r += 2) {
-            const ulonglong2 x0 = __ldg(reinterpret_cast<const ulonglong2 *>(k0 + r));
-            const ulonglong2 x1 = __ldg(reinterpret_cast<const ulonglong2 *>(k1 + r));
-            acc0[r] = add_mod(acc0[r], mred(v[r], x0.x, q, md.qinv), q);
-            acc0[r + 1] = add_mod(acc0[r + 1], mred(v[r + 1], x0.y, q, md.qinv), q);
-            acc1[r] = add_mod(acc1[r], mred(v[r], x1.x, q, md.qinv), q);
-            acc1[r + 1] = add_mod(acc1[r + 1], mred(v[r + 1], x1.y, q, md.qinv), q);
+        for (int k = 0; k < 8; ++k) {
+            acc0[k * T] = add_mod(acc0[k * T], mred(v[k], __ldg(k0 + k * T), q, md.qinv), q);
+            acc1[k * T] = add_mod(acc1[k * T], mred(v[k], __ldg(k1 + k * T), q, md.qinv), q);
         }
     }
     uint64_t *o0 = g.out + (long long)grp * g.out_gstride + (long long)sidx * g.out_istride +
-                   (long long)l * N + base;
+                   (long long)l * N + rowoff + t;
     uint64_t *o1 = o0 + g.out_ostride;
 #pragma unroll
-    for (int r = 0; r < 8; r += 2) {
-        *reinterpret_cast<ulonglong2 *>(o0 + r) = make_ulonglong2(acc0[r], acc0[r + 1]);
-        *reinterpret_cast<ulonglong2 *>(o1 + r) = make_ulonglong2(acc1[r], acc1[r + 1]);
+    for (int k = 0; k < 8; ++k) {
+        o0[k * T] = acc0[k * T];
+        o1[k * T] = acc1[k * T];
     }
 }
 
@@ -1180,7 +1130,7 @@ void ntt_prepare(const Context &c) {
 }
 
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
-                        uint64_t *tbuf, cudaStream_t st) {
+                        cudaStream_t st) {
     const int L1 = src.level + 1, limbs = L1 + c.nP;
     const int np = npolys * src.ndigits;
     if (np <= 0) return;
@@ -1198,11 +1148,8 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
     const int max_polys = std::max(src.ndigits, (65535 / limbs) / src.ndigits * src.ndigits);
     for (int p0 = 0; p0 < np; p0 += max_polys) {
         const int npp = std::min(max_polys, np - p0);
-        // column pass: tbuf (column-major); row pass: tbuf -> out
-        NttArgs b = a, bt = a;
+        NttArgs b = a;
         b.ls.base = out + (long long)p0 * a.ls.poly_stride;
-        b.in_t = tbuf + (long long)p0 * a.ls.poly_stride;
-        bt.ls.base = tbuf + (long long)p0 * a.ls.poly_stride;
         DigitSrc sb = src;
         const int first_poly = p0 / src.ndigits;
         sb.x = src.x + (long long)first_poly * src.x_pstride;
@@ -1230,7 +1177,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
-            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(bt, sb);                                 \
+            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(b, sb);                                  \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \

@@ -58,14 +58,12 @@ struct DigitIpArgs {
     long long out_gstride = 0, out_istride = 0, out_ostride = 0;
 };
 // Column pass of the digits (as ntt_forward_digits) then the fused row pass
-// + inner product; logN 13..16.  dig receives the column-pass output
-// (column-major limbs).
+// + inner product; logN 13..16.  dig receives the column-pass output.
 void ntt_forward_digits_ip(const Context &c, const DigitSrc &src, uint64_t *dig, int npolys,
                            const DigitIpArgs &ip, cudaStream_t st);
-// NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load;
-// tbuf (as large as out) holds the column pass's column-major output.
+// NTT of the gadget digits [poly][digit][level+1+nP][N] reconstructed on load.
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
-                        uint64_t *tbuf, cudaStream_t st);
+                        cudaStream_t st);
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
 // Sets the kernels' launch attributes for c's device (idempotent); called
 // before a stream capture so that nothing but launches happens inside it.
