@@ -206,6 +206,7 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
     t.nt = (int)tgt.size();
     std::vector<uint64_t> inv(t.ns), qmod((size_t)t.nt * t.ns), vq((size_t)t.nt * (t.ns + 1));
     std::vector<double> qmodd((size_t)t.nt * t.ns * 2);
+    std::vector<uint64_t> negq(t.nt);
     t.fp_src = 1;
     for (int i = 0; i < t.ns; ++i)
         if (all[src[i]] >= kFp64Bound) t.fp_src = 0;
@@ -227,6 +228,7 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
         uint64_t pk = all[tgt[k]], qmodp = 1;
         for (int j = 0; j < t.ns; ++j) qmodp = h_mulmod(qmodp, all[src[j]] % pk, pk);
         uint64_t v = pk - qmodp;
+        negq[k] = h_mform(v % pk, pk);
         uint64_t *row = &vq[(size_t)k * (t.ns + 1)];
         row[0] = 0;
         for (int i = 1; i <= t.ns; ++i) {
@@ -239,6 +241,7 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
     t.qmod = upload(qmod);
     t.vq = upload(vq);
     t.qmodd = upload(qmodd);
+    t.negq = upload(negq);
     return t;
 }
 

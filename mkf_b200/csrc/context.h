@@ -21,6 +21,7 @@ struct ModUpTab {
     const uint64_t *inv = nullptr;   // [ns]      MForm((Q/q_i)^-1 mod q_i)
     const uint64_t *qmod = nullptr;  // [nt][ns]  MForm(Q/q_i mod p_j)
     const uint64_t *vq = nullptr;    // [nt][ns+1] v*(p_j - Q mod p_j) mod p_j
+    const uint64_t *negq = nullptr;  // [nt]      MForm(-Q mod p_j)
     // float64 form for sources and targets below 2^50: [nt][ns] pairs
     // (Q/q_i mod p_j, that / p_j); fp_src = every source modulus below 2^50
     const double *qmodd = nullptr;

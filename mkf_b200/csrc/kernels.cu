@@ -369,9 +369,12 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
         modup_kernel<64><<<grid, kBlock, 0, st>>>(a);
 }
 
-// Summed ModUp: a thread owns one coefficient of one output polynomial and a
-// chunk of CH target limbs, and walks the terms, reconstructing each term's
-// y_i and correction once per chunk.
+// Summed ModUp: out = sum over terms of ModUp(term) mod p, canonical.  Every
+// term's ModUp is sum_i y_i (Q/q_i) - v Q mod p (reconstructRNS + multSum,
+// basis_extension.go:537-646), which is linear in (y, v): a thread owns one
+// coefficient of one output polynomial and a chunk of target limbs, adds the
+// terms' y_i (each sum kept below q_i, a wrap counting one more Q) and
+// corrections, and forms one multSum per target from the sums.
 
 struct ModUpSumArgs {
     ModUpTab tab;
@@ -384,35 +387,52 @@ struct ModUpSumArgs {
     int row0, nt, N, terms, nchunks;
 };
 
-template <int MAXNS, int CH>
-__global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a) {
+template <int MAXNS>
+__global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a, int ch) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.N) return;
-    const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * CH;
-    const int nj = min(CH, a.nt - j0);
-    uint64_t acc[CH];
+    const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * ch;
+    const int nj = min(ch, a.nt - j0);
+    const int ns = a.tab.ns;
+    // Y_i = sum over terms of y_i, kept below q_i; each wrap adds q_i, i.e.
+    // Q to the reconstructed value, counted in wraps
+    uint64_t Y[MAXNS];
 #pragma unroll
-    for (int jj = 0; jj < CH; ++jj) acc[jj] = 0;
+    for (int i = 0; i < MAXNS; ++i) Y[i] = 0;
+    uint64_t vsum = 0, wraps = 0;
     for (int t = 0; t < a.terms; ++t) {
         const uint64_t *src = a.src + (long long)t * a.src_tstride + (long long)p * a.src_pstride;
         uint64_t xs[MAXNS], y[MAXNS];
 #pragma unroll
         for (int i = 0; i < MAXNS; ++i)
-            if (i < a.tab.ns) xs[i] = src[(long long)i * a.N + x];
-        const uint64_t v = reconstruct<MAXNS>(xs, a.tab, a.mods, y);
+            if (i < ns) xs[i] = src[(long long)i * a.N + x];
+        vsum += reconstruct<MAXNS>(xs, a.tab, a.mods, y);
 #pragma unroll
-        for (int jj = 0; jj < CH; ++jj) {
-            if (jj < nj) {
-                const DevModulus &m = a.mods[a.tgt(j0 + jj)];
-                acc[jj] = add_mod(acc[jj], canon(multsum<MAXNS>(y, a.tab, a.row0 + j0 + jj, v, m), m.q),
-                                  m.q);
+        for (int i = 0; i < MAXNS; ++i) {
+            if (i < ns) {
+                const uint64_t qi = a.mods[a.tab.src_mod[i]].q;
+                const uint64_t s = Y[i] + y[i];
+                const bool w = s >= qi;
+                Y[i] = w ? s - qi : s;
+                wraps += w;
             }
         }
     }
     uint64_t *out = a.out + (long long)p * a.out_pstride + (long long)j0 * a.N + x;
+    for (int jj = 0; jj < nj; ++jj) {
+        const int row = a.row0 + j0 + jj;
+        const DevModulus &m = a.mods[a.tgt(j0 + jj)];
+        const uint64_t *qm = a.tab.qmod + (size_t)row * ns;
+        uint64_t lo = 0, hi = 0;
 #pragma unroll
-    for (int jj = 0; jj < CH; ++jj)
-        if (jj < nj) out[(long long)jj * a.N] = acc[jj];
+        for (int i = 0; i < MAXNS; ++i)
+            if (i < ns) mac128(lo, hi, Y[i], __ldg(qm + i));
+        // + vsum * (-Q) + wraps * Q, Montgomery forms
+        const uint64_t nq = __ldg(a.tab.negq + row);
+        mac128(lo, hi, vsum, nq);
+        mac128(lo, hi, wraps, nq ? m.q - nq : 0);
+        out[(long long)jj * a.N] = mred128(hi, lo, m.q, m.qinv);
+    }
 }
 
 void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src,
@@ -427,25 +447,16 @@ void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src
     ProfScope ps(c, PK_MODUP, st, 8.0 * c.N * npolys * ((double)tab.ns * terms + nt));
     const dim3 grid = grid_for(c.N, npolys * nchunks);
     note_launch();
-#define MKF_SUM_NS(CH)                                                                             \
-    if (tab.ns <= 4)                                                                               \
-        modup_sum_kernel<4, CH><<<grid, kBlock, 0, st>>>(a);                                        \
-    else if (tab.ns <= 8)                                                                          \
-        modup_sum_kernel<8, CH><<<grid, kBlock, 0, st>>>(a);                                        \
-    else if (tab.ns <= 16)                                                                         \
-        modup_sum_kernel<16, CH><<<grid, kBlock, 0, st>>>(a);                                       \
-    else if (tab.ns <= 32)                                                                         \
-        modup_sum_kernel<32, CH><<<grid, kBlock, 0, st>>>(a);                                       \
-    else                                                                                           \
-        modup_sum_kernel<64, CH><<<grid, kBlock, 0, st>>>(a);
-    if (ch == 8) {
-        MKF_SUM_NS(8)
-    } else if (ch == 24) {
-        MKF_SUM_NS(24)
-    } else {
-        MKF_SUM_NS(12)
-    }
-#undef MKF_SUM_NS
+    if (tab.ns <= 4)
+        modup_sum_kernel<4><<<grid, kBlock, 0, st>>>(a, ch);
+    else if (tab.ns <= 8)
+        modup_sum_kernel<8><<<grid, kBlock, 0, st>>>(a, ch);
+    else if (tab.ns <= 16)
+        modup_sum_kernel<16><<<grid, kBlock, 0, st>>>(a, ch);
+    else if (tab.ns <= 32)
+        modup_sum_kernel<32><<<grid, kBlock, 0, st>>>(a, ch);
+    else
+        modup_sum_kernel<64><<<grid, kBlock, 0, st>>>(a, ch);
 }
 
 // ----------------------------------------------------------------------------

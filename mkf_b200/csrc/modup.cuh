@@ -52,6 +52,13 @@ MKF_DEV uint64_t multsum(const uint64_t *y, const ModUpTab &tab, int row, uint64
     return hi - h + pm.q + tab.vq[(size_t)row * (tab.ns + 1) + v];
 }
 
+// (lo, hi) += a * b on 128 bits
+MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
+    asm("mad.lo.cc.u64 %0, %2, %3, %0;\n\tmadc.hi.u64 %1, %2, %3, %1;"
+        : "+l"(lo), "+l"(hi)
+        : "l"(a), "l"(b));
+}
+
 MKF_DEV uint64_t canon(uint64_t x, uint64_t q) {
     while (x >= q) x -= q;
     return x;

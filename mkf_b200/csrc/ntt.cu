@@ -592,12 +592,6 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
 }
 
-// (lo, hi) += a * b on 128 bits
-MKF_DEV void mac128(uint64_t &lo, uint64_t &hi, uint64_t a, uint64_t b) {
-    asm("mad.lo.cc.u64 %0, %2, %3, %0;\n\tmadc.hi.u64 %1, %2, %3, %1;"
-        : "+l"(lo), "+l"(hi)
-        : "l"(a), "l"(b));
-}
 
 // Column pass of the NTT of gadget digits with the decomposition fused into
 // its first radix-8 pass.  Every column of a digit limb belongs to T = S/8
