@@ -352,6 +352,31 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
             }
         }
     }
+    // The phase kernels (n2 > 0) read the tables in pass order: within stage
+    // st = 3p + u of a transform of 2^n points (radix-8 passes of D stages,
+    // the last one possibly shorter; ps = max(n - 3p - 3, 0)), entry
+    // i = tb << a | rb (a = 3 - D + u) moves to rb << (st - a) | tb, so that
+    // the lanes of a warp, which differ in tb, read consecutive entries.
+    auto pass_order = [](Tw *tab, int n) {
+        std::vector<Tw> tmp;
+        for (int st = 1; st < n; ++st) {
+            const int p = st / 3, u = st % 3;
+            const int ps = std::max(n - 3 * p - 3, 0), D = n - 3 * p - ps, a = 3 - D + u;
+            tmp.assign(tab + (1 << st), tab + (2 << st));
+            for (int i = 0; i < (1 << st); ++i)
+                tab[(1 << st) + (((i & ((1 << a) - 1)) << (st - a)) | (i >> a))] = tmp[i];
+        }
+    };
+    if (n2) {
+        for (int m = 0; m < nmods; ++m) {
+            pass_order(&fwd1[(size_t)m * S1], n1);
+            pass_order(&inv1[(size_t)m * S1], n1);
+            for (int h = 0; h < S1; ++h) {
+                pass_order(&fwd2[(size_t)m * N + (size_t)h * (1 << n2)], n2);
+                pass_order(&inv2[(size_t)m * N + (size_t)h * (1 << n2)], n2);
+            }
+        }
+    }
     d_mods = upload(h_mods);
     d_fwd1 = upload(fwd1);
     d_inv1 = upload(inv1);

@@ -322,6 +322,17 @@ template <int LOGS> MKF_DEV int elem(int p, int t, int r) {
     return ((t >> ps) << (ps + 3)) | (r << ps) | (t & ((1 << ps) - 1));
 }
 
+// Position of the twiddle of stage st = 3p + u used by register r of thread
+// t.  The phase tables store each stage's entries in pass order (see the
+// context's table construction): the stage's index i = (t >> ps) << a | rb,
+// rb = r >> (D - u) the part chosen by the register, sits at rb * 2^(st-a) +
+// (t >> ps), so that the lanes of a warp read consecutive entries.
+template <int LOGS> MKF_DEV int twpos(int p, int u, int t, int r) {
+    const int st = 3 * p + u, ps = pass_pos<LOGS>(p);
+    const int D = LOGS - 3 * p - ps, a = 3 - D + u;
+    return (1 << st) + ((r >> (D - u)) << (st - a)) + (t >> ps);
+}
+
 MKF_DEV Tw ldtw(const Tw *p) {
     const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2 *>(p));
     return Tw{v.x, v.y};
@@ -418,8 +429,8 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
-                    const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
-                    const Tw w = TWS ? ldtw_s(tw + (1 << st) + i) : ldtw(tw + (1 << st) + i);
+                    const int i = twpos<LOGS>(p, u, t, r);
+                    const Tw w = TWS ? ldtw_s(tw + i) : ldtw(tw + i);
                     if (LAZY)
                         ct_bfly_lazy(v[r], v[r + stride], w, q);
                     else
@@ -461,8 +472,8 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
-                    const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
-                    const TwD w = TWS ? ldtwd_s(tw + (1 << st) + i) : ldtwd(tw + (1 << st) + i);
+                    const int i = twpos<LOGS>(p, u, t, r);
+                    const TwD w = TWS ? ldtwd_s(tw + i) : ldtwd(tw + i);
                     ct_bfly_f(v[r], v[r + stride], w, q);
                 }
             }
@@ -761,11 +772,11 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
                         U = x;
                         V = y;
                     } else {
-                        const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
+                        const int i = twpos<LOGS>(p, u, t, r);
                         if (LAZY)
-                            gs_bfly_lazy(U, V, ldtw(tw + (1 << st) + i), q, bias);
+                            gs_bfly_lazy(U, V, ldtw(tw + i), q, bias);
                         else
-                            gs_bfly(U, V, ldtw(tw + (1 << st) + i), q);
+                            gs_bfly(U, V, ldtw(tw + i), q);
                     }
                 }
             }
@@ -802,8 +813,7 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
                         V = mulmod_f(__dadd_rn(U, -V), md.lastd, md.lastq, q);
                         U = x;
                     } else {
-                        const int i = elem<LOGS>(p, t, r) >> (LOGS - st);
-                        gs_bfly_f(U, V, ldtwd(tw + (1 << st) + i), q, qi);
+                        gs_bfly_f(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
                     }
                 }
             }
