@@ -387,10 +387,12 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
     // float64 twiddles (w, w/q) for the limbs below 2^50; the tables cover
     // every modulus so that they index like the integer ones
     auto to_f = [&](const std::vector<Tw> &t, size_t per) {
+        // centered: |w| <= q/2, so that |w/q| <= 1/2
         std::vector<TwD> o(t.size());
         for (size_t i = 0; i < t.size(); ++i) {
-            const double q = (double)all[i / per];
-            o[i] = TwD{(double)t[i].w, (double)t[i].w / q};
+            const uint64_t qq = all[i / per];
+            const long long w = t[i].w > qq / 2 ? (long long)t[i].w - (long long)qq : (long long)t[i].w;
+            o[i] = TwD{(double)w, (double)w / (double)qq};
         }
         return o;
     };

@@ -86,10 +86,8 @@ __device__ __forceinline__ void gs_bfly_lazy(uint64_t &U, uint64_t &V, const Tw 
     U = x;
 }
 
-// Float64 Cooley-Tukey butterfly (mulmod_f): from |U|, |V| <= B*q the
-// outputs stay below (B + 1/2 + B/8) q for q < 2^50, so a radix-8 pass of
-// three stages that starts from centered words (B = 1/2) keeps every V
-// operand below 2q (the rounding trick's range) and ends below 2.5q.
+// Float64 Cooley-Tukey butterfly (mulmod_f); the bounds it keeps are those
+// of fsched below.
 __device__ __forceinline__ void ct_bfly_f(double &U, double &V, const TwD w, double q) {
     const double t = mulmod_f(V, w.w, w.wq, q);
     const double u = U;
@@ -449,14 +447,56 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
     }
 }
 
-// The passes of a forward phase in float64 (limbs below 2^50): the tile holds
-// the bits of centered doubles, and every pass ends by reducing its words to
-// |x| <= q/2, so that the next pass (or phase) starts centered again.  KEEP:
-// the last pass leaves its words in vout, centered.
-template <int LOGS, bool KEEP = false, bool TWS = false, bool REGIN = false>
+// Word bounds of the float64 forward passes, in units of q.  With twiddles
+// stored centered (|w| <= q/2, so |w/q| <= 1/2) and |V| <= 4q, mulmod_f's
+// quotient is within 1/2 + |V|/(16q) of V*w/q (q < 2^50), so a butterfly
+// maps a bound b to b + 1/2 + b/16, the rounding trick's product stays below
+// 2^51 and the words below 8q < 2^53.  The passes reduce their words
+// (reduce_f, back to q/2) only where the next pass or the caller needs it:
+// the greedy schedule below, evaluated at compile time from the input bound
+// IN16/16 and the required output bound OUT16/16.
+namespace fsched {
+constexpr double grow(double b) { return b + 0.5 + b / 16 + 1.0 / 1024; }
+constexpr double kVmax = 3.9, kRed = 0.5 + 1.0 / 1024;
+// bound after D stages from b, or -1 if a V operand would exceed kVmax
+constexpr double run(double b, int D) {
+    for (int i = 0; i < D; ++i) {
+        if (b > kVmax) return -1.0;
+        b = grow(b);
+    }
+    return b;
+}
+constexpr int stages(int LOGS, int p) { return LOGS - 3 * p < 3 ? LOGS - 3 * p : 3; }
+// bit p: reduce after pass p; bit 31: reduce the input first
+constexpr unsigned mask(int LOGS, int in16, int out16) {
+    const int NP = (LOGS + 2) / 3;
+    unsigned m = 0;
+    double b = in16 / 16.0;
+    if (run(b, stages(LOGS, 0)) < 0) {
+        m |= 1u << 31;
+        b = kRed;
+    }
+    for (int p = 0; p < NP; ++p) {
+        b = run(b, stages(LOGS, p));
+        const bool red = p + 1 < NP ? run(b, stages(LOGS, p + 1)) < 0 : b > out16 / 16.0;
+        if (red) {
+            m |= 1u << p;
+            b = kRed;
+        }
+    }
+    return m;
+}
+} // namespace fsched
+
+// The passes of a forward phase in float64 (limbs below 2^50) on the bits of
+// doubles in the tile, with the reductions of fsched::mask.  KEEP: the last
+// pass leaves its words in vout; REGIN: the first pass takes its words
+// (points elem(0, t, r)) from vout.
+template <int LOGS, int IN16, int OUT16, bool KEEP = false, bool TWS = false, bool REGIN = false>
 MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c, int t,
                           double *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    constexpr unsigned RED = fsched::mask(LOGS, IN16, OUT16);
     double v[8];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
@@ -464,6 +504,10 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
         for (int r = 0; r < 8; ++r)
             v[r] = (REGIN && p == 0) ? vout[r]
                                      : __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+        if (p == 0 && (RED >> 31)) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
+        }
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const int st = 3 * p + u;
@@ -478,8 +522,10 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
                 }
             }
         }
+        if ((RED >> p) & 1) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
+            for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
+        }
         if (KEEP && p == NP - 1) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) vout[r] = v[r];
@@ -527,7 +573,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
             const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-            fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+            fwd_passes_f<LOGS, 32, 8, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
             for (int k = 0; k < 8; ++k)
                 data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
@@ -563,7 +609,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     }
     __syncthreads();
     if (fp)
-        fwd_passes_f<LOGS, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
+        fwd_passes_f<LOGS, 8, 32, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
     else if (lazy)
         fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
     else
@@ -605,142 +651,168 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
 
 
 // Column pass of the NTT of gadget digits with the decomposition fused into
-// its first radix-8 pass.  Every column of a digit limb belongs to T = S/8
-// lanes of one warp, so the pass needs no block-wide barrier: a multSum word
-// (basis_extension.go:581-646) is rebuilt from the digit's y_i and float64
-// correction v, which the prep kernel stores column-major (coefficient
-// r*2^n2 + cc at cc*2^n1 + r), straight into the registers of the first
-// pass; the block's transformed columns are stored row-major through the
-// tile, for the row pass.  One-limb digits and own limbs without an NTT-domain
-// copy are reduced from the coefficient-domain input instead, through a
-// shared-memory tile.  Own limbs with an NTT-domain input are copied, in the
-// standard layout, to src.own_out.  Grid rows enumerate (poly, digit, limb).
-// The integer multSum's 128-bit sum needs no reduction on the way: its high
-// word stays below ns * q_i * p_j / 2^64 < p_j.
+// its first radix-8 pass.  A block owns C = 2048 / S columns (T = S/8 lanes
+// per column) of one (poly, digit) and walks every target limb:
+// the digit's y_i and float64 corrections for those columns (stored
+// column-major by the prep kernel, coefficient r*2^n2 + cc at cc*2^n1 + r,
+// so the block's columns are contiguous) are staged in shared memory once,
+// and for each limb a multSum word (basis_extension.go:581-646) is rebuilt
+// from them straight into the registers of the first pass.  The transformed
+// columns are stored row-major through the exchange tile, for the row pass.
+// One-limb digits are reduced from the coefficient-domain source limb (staged
+// once); own limbs are copied from the NTT-domain input (src.own) or, without
+// one, reduced from the source limb.  The integer multSum's 128-bit sum needs
+// no reduction on the way: its high word stays below ns * q_i * p_j / 2^64.
+constexpr int kColThreads = 256, kColWords = 2048;
+// dynamic shared memory for alpha staged limbs (alpha <= 8: 146 KB); the
+// kernel's attribute is set once for alpha = 8
+inline size_t digits_col_smem(int alpha) {
+    return (size_t)kColWords * 8 * (1 + std::max(alpha, 1)) + kColWords;
+}
+
 template <int LOGS>
-__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
-    constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    __shared__ uint64_t s[kTile];
-    __shared__ __align__(16) uint64_t twsm[2 * S]; // the column table (Tw or TwD)
+__global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
+    constexpr int S = 1 << LOGS, T = S / 8, C = kColWords / S, NW = kColWords;
+    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t *s = dsm;                 // exchange tile, C columns
+    uint64_t *ys = dsm + NW;           // [alpha][C][S] staged y_i (or the one-limb source)
+    uint8_t *vs = reinterpret_cast<uint8_t *>(ys + (size_t)NW * max(src.alpha, 1));
     const int limbs = a.ls.limbs;
-    const int pd = blockIdx.y / limbs, l = blockIdx.y % limbs;
-    const int poly = pd / src.ndigits, d = pd % src.ndigits;
-    const int m = a.ls.mod_of(l);
-    const DevModulus md = a.mods[m];
-    const uint64_t q = md.q;
+    const int pd = blockIdx.y, poly = pd / src.ndigits, d = pd % src.ndigits;
     const int N = 1 << a.logN, R = 1 << a.n2;
     const int L1 = src.level + 1;
     const int start = d * src.alpha;
     const int ns = digit_ns(src.level, src.alpha, d);
-    const bool own_limb = l < L1 && l >= start && l < start + ns;
-    const int mode = ns == 1 ? 0 : own_limb ? 1 : 2;
+    const bool msum = ns >= 2 && src.tabs;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
-    if (own_limb && src.own.p[0]) {
-        // the digit's own limb is the input limb itself: copy its NTT form,
-        // unless the fused row pass reads it from the input directly
-        if (src.own_skip) return;
-        const int gp = src.poly0 + poly;
-        const uint64_t *xn = (gp < src.own.split
-                                  ? src.own.p[0] + (long long)gp * src.own.pstride[0]
-                                  : src.own.p[1] + (long long)(gp - src.own.split) * src.own.pstride[1]) +
-                             (long long)l * N;
-        uint64_t *dst = src.own_out + (long long)pd * a.ls.poly_stride + (long long)l * N;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int idx = e * kPhaseThreads + tid;
-            const int coef = blockIdx.x * C + (idx / C) * R + idx % C;
-            dst[coef] = xn[coef];
+    const int col0 = blockIdx.x * C;
+    // stage the digit's sources for the block's columns
+    if (msum) {
+        const ulonglong2 *yg = reinterpret_cast<const ulonglong2 *>(src.y + (long long)pd * src.alpha * N +
+                                                                   (long long)col0 * S);
+        for (int i = 0; i < ns; ++i)
+            for (int e = tid; e < NW / 2; e += kColThreads)
+                reinterpret_cast<ulonglong2 *>(ys + (size_t)i * NW)[e] = __ldg(yg + (size_t)i * N / 2 + e);
+        const uint4 *vg = reinterpret_cast<const uint4 *>(src.v + (long long)pd * N + (long long)col0 * S);
+        for (int e = tid; e < NW / 16; e += kColThreads) reinterpret_cast<uint4 *>(vs)[e] = __ldg(vg + e);
+    } else if (ns == 1) {
+        const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)start * N;
+        for (int idx = tid; idx < NW; idx += kColThreads) {
+            const int r = idx / C, cc = idx % C;
+            ys[cc * S + r] = xs[(long long)r * R + col0 + cc];
         }
-        return;
     }
-    // float64 limbs (below 2^50): the words enter the transform as centered
-    // doubles and leave it as doubles for the row pass
-    const bool fp = q < kFp64Bound;
-    {
-        const uint64_t *tsrc = fp ? reinterpret_cast<const uint64_t *>(a.tw1d + (size_t)m * S)
-                                  : reinterpret_cast<const uint64_t *>(a.tw1 + (size_t)m * S);
-        for (int i = tid; i < 2 * S; i += kPhaseThreads) twsm[i] = __ldg(tsrc + i);
-    }
-    const int col = blockIdx.x * C + c;
-    // first-pass words (points r*T + t of column col): canonical words, or
-    // the bits of centered doubles for float64 limbs
-    uint64_t vi[8];
-    if (mode == 2) {
-        const ModUpTab *tb = src.tabs + d * (src.alpha + 1) + ns;
-        const int row = l < L1 ? l : src.nQ + (l - L1);
-        const uint64_t *yp = src.y + (long long)pd * src.alpha * N + (long long)col * S + t;
-        const uint8_t *vp = src.v + (long long)pd * N + (long long)col * S + t;
-        const uint64_t *tvr = tb->vq + row * (ns + 1);
-        if (fp && tb->fp_src) {
-            // float64 multSum: each y_i * (Q/q_i mod p) reduced by mulmod_f
-            // (|.| <= 5p/8), the terms and the correction summed, then centered
-            double acc[8];
+    __syncthreads();
+    const ModUpTab *tb = msum ? src.tabs + d * (src.alpha + 1) + ns : nullptr;
+    for (int l = 0; l < limbs; ++l) {
+        const bool own_limb = l < L1 && l >= start && l < start + ns;
+        uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
+        if (own_limb && src.own.p[0]) {
+            // the digit's own limb is the input limb itself: copy its NTT
+            // form, unless the fused row pass reads it from the input directly
+            if (src.own_skip) continue;
+            const int gp = src.poly0 + poly;
+            const uint64_t *xn = (gp < src.own.split
+                                      ? src.own.p[0] + (long long)gp * src.own.pstride[0]
+                                      : src.own.p[1] + (long long)(gp - src.own.split) * src.own.pstride[1]) +
+                                 (long long)l * N + col0;
+            uint64_t *od = src.own_out + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
+            for (int idx = tid; idx < NW; idx += kColThreads) {
+                const long long o = (long long)(idx / C) * R + idx % C;
+                od[o] = xn[o];
+            }
+            continue;
+        }
+        const int m = a.ls.mod_of(l);
+        const DevModulus md = a.mods[m];
+        const uint64_t q = md.q;
+        const bool fp = q < kFp64Bound;
+        // first-pass words (points r*T + t of column c): canonical words, or
+        // the bits of centered doubles for float64 limbs
+        uint64_t vi[8];
+        if (own_limb) {
+            // own limb without an NTT-domain copy: MRed(x_l, 2^64 mod q)
+            const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)l * N;
+            for (int idx = tid; idx < NW; idx += kColThreads) {
+                const int r = idx / C, cc = idx % C;
+                s[saddr<S>(cc, r)] = mred(xs[(long long)r * R + col0 + cc], md.mont1, q, md.qinv);
+            }
+            __syncthreads();
 #pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            for (int i = 0; i < ns; ++i) {
-                const double cw = __ldg(tb->qmodd + (row * ns + i) * 2);
-                const double cq = __ldg(tb->qmodd + (row * ns + i) * 2 + 1);
-                const uint64_t *yi = yp + (long long)i * N;
+            for (int r = 0; r < 8; ++r) {
+                const uint64_t x = s[saddr<S>(c, elem<LOGS>(0, t, r))];
+                vi[r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+            }
+        } else if (!msum) {
+            // one-limb digit: MRed(x_start, 2^64 mod q)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint64_t x = mred(ys[c * S + r * T + t], md.mont1, q, md.qinv);
+                vi[r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+            }
+        } else {
+            const int row = l < L1 ? l : src.nQ + (l - L1);
+            const uint64_t *tvr = tb->vq + row * (ns + 1);
+            const uint64_t *yl = ys + c * S + t;
+            const uint8_t *vl = vs + c * S + t;
+            if (fp && tb->fp_src) {
+                // float64 multSum: each y_i * (Q/q_i mod p) reduced by
+                // mulmod_f (|.| <= 5p/8), the terms and the correction
+                // summed, then centered
+                double acc[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                for (int i = 0; i < ns; ++i) {
+                    const double cw = __ldg(tb->qmodd + (row * ns + i) * 2);
+                    const double cq = __ldg(tb->qmodd + (row * ns + i) * 2 + 1);
+#pragma unroll
+                    for (int r = 0; r < 8; ++r)
+                        acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(yl[i * NW + r * T]), cw, cq, md.qd));
+                }
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
-                    acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(__ldg(yi + r * T)), cw, cq, md.qd));
-            }
+                    vi[r] = (uint64_t)__double_as_longlong(
+                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + vl[r * T]))), md.qinvd, md.qd));
+            } else {
+                // integer multSum, four words at a time
 #pragma unroll
-            for (int r = 0; r < 8; ++r)
-                vi[r] = (uint64_t)__double_as_longlong(
-                    reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + __ldg(vp + r * T)))), md.qinvd, md.qd));
-        } else {
-            // integer multSum, four words at a time
+                for (int h = 0; h < 8; h += 4) {
+                    uint64_t lo[4], hi[4];
 #pragma unroll
-            for (int h = 0; h < 8; h += 4) {
-                uint64_t lo[4], hi[4];
+                    for (int r = 0; r < 4; ++r) lo[r] = hi[r] = 0;
+                    for (int i = 0; i < ns; ++i) {
+                        const uint64_t b = __ldg(tb->qmod + row * ns + i);
 #pragma unroll
-                for (int r = 0; r < 4; ++r) lo[r] = hi[r] = 0;
-                for (int i = 0; i < ns; ++i) {
-                    const uint64_t b = __ldg(tb->qmod + row * ns + i);
-                    const uint64_t *yi = yp + (long long)i * N + h * T;
+                        for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], yl[i * NW + (h + r) * T], b);
+                    }
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], __ldg(yi + r * T), b);
-                }
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
-                    const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + __ldg(vp + (h + r) * T)), q);
-                    vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+                    for (int r = 0; r < 4; ++r) {
+                        const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
+                        const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + vl[(h + r) * T]), q);
+                        vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
+                    }
                 }
             }
         }
-    } else {
-        // coefficient-domain source limb, transposed through the tile
-        const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)(mode == 0 ? start : l) * N;
+        // the column table of this limb, read in pass order from global memory
+        if (fp) {
+            double vf[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int idx = e * kPhaseThreads + tid;
+            for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)vi[r]);
+            fwd_passes_f<LOGS, 8, 32, false, false, true>(s, a.tw1d + (size_t)m * S, md.qd, md.qinvd, c, t, vf);
+        } else if (q < kLazyBound) {
+            fwd_passes<LOGS, true, false, false, true>(s, a.tw1 + (size_t)m * S, q, c, t, vi);
+        } else {
+            fwd_passes<LOGS, false, false, false, true>(s, a.tw1 + (size_t)m * S, q, c, t, vi);
+        }
+        // the tile holds every column of the block: store it row-major
+        __syncthreads();
+        for (int idx = tid; idx < NW; idx += kColThreads) {
             const int r = idx / C, cc = idx % C;
-            s[saddr<S>(cc, r)] = mred(xs[blockIdx.x * C + r * R + cc], md.mont1, q, md.qinv);
+            dst[(long long)r * R + cc] = s[saddr<S>(cc, r)];
         }
         __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const uint64_t x = s[saddr<S>(c, elem<LOGS>(0, t, r))];
-            vi[r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
-        }
     }
-    __syncthreads(); // the staged table
-    if (fp) {
-        double vf[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)vi[r]);
-        fwd_passes_f<LOGS, false, true, true>(s, reinterpret_cast<const TwD *>(twsm), md.qd, md.qinvd, c, t, vf);
-    } else if (q < kLazyBound) {
-        fwd_passes<LOGS, true, false, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
-    } else {
-        fwd_passes<LOGS, false, false, true, true>(s, reinterpret_cast<const Tw *>(twsm), q, c, t, vi);
-    }
-    // the tile holds every column of the block: store it row-major
-    __syncthreads();
-    tile_store<LOGS, true>(s, a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N, R, tid, md,
-                           kRedNone);
 }
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
@@ -1021,10 +1093,15 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
                 double vf[8];
 #pragma unroll
                 for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
-                fwd_passes_f<LOGS, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+                // words below 4q: x + 4q is a non-negative integer below 2^53,
+                // which MRed takes as it is
+                fwd_passes_f<LOGS, 32, 64, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+                const double off = 4.0 * md.qd + MKF_F_2P52;
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
-                    v[k] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
+                    v[k] = (uint64_t)__double_as_longlong(
+                               __dadd_rn(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), off)) -
+                           0x4330000000000000ull;
             } else {
                 if (lazy)
                     fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
@@ -1102,9 +1179,10 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             sb.v = src.v + (long long)p0 * c.N;                                                    \
             sb.poly0 = first_poly;                                                                 \
             sb.own_out = b.ls.base;                                                                \
-            dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs);                                     \
+            dim3 g1((1 << L2G) / (kColWords >> L1G), npp);                                         \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
-            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(b, sb);                                  \
+            smem_attr(ntt_fwd_digits_col<L1G>, c.device, digits_col_smem(8));                  \
+            ntt_fwd_digits_col<L1G><<<g1, kColThreads, digits_col_smem(src.alpha), st>>>(b, sb);   \
             if (p0) note_launch(1);                                                                \
         }                                                                                          \
         dim3 g2((1 << L1G) / (kTile >> L2G), limbs, ip.groups * ip.nin);                           \
@@ -1130,6 +1208,9 @@ void ntt_prepare(const Context &c) {
     smem_attr(ntt_fwd_phase<7, false>, c.device, fwd_phase_smem<7, false>());
     smem_attr(ntt_fwd_phase<8, false>, c.device, fwd_phase_smem<8, false>());
     smem_attr(ntt_digits_row_ip<7>, c.device, kRowIpSmem);
+    smem_attr(ntt_fwd_digits_col<6>, c.device, digits_col_smem(8));
+    smem_attr(ntt_fwd_digits_col<7>, c.device, digits_col_smem(8));
+    smem_attr(ntt_fwd_digits_col<8>, c.device, digits_col_smem(8));
     smem_attr(ntt_digits_row_ip<8>, c.device, kRowIpSmem);
 }
 
@@ -1178,10 +1259,11 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         switch (c.logN) {
 #define MKF_DIGITS_CASE(LN, L1G, L2G)                                                              \
     case LN: {                                                                                     \
-        dim3 g1((1 << L2G) / (kTile >> L1G), npp * limbs), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
+        dim3 g1((1 << L2G) / (kColWords >> L1G), npp), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
-            ntt_fwd_digits_col<L1G><<<g1, block, 0, st>>>(b, sb);                                  \
+            smem_attr(ntt_fwd_digits_col<L1G>, c.device, digits_col_smem(8));                  \
+            ntt_fwd_digits_col<L1G><<<g1, kColThreads, digits_col_smem(src.alpha), st>>>(b, sb);   \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \
