@@ -51,6 +51,9 @@ def parse():
                     help="products in the mixed batch (k in {2,4,8,16}, logN in {14,15}, "
                          "level uniform over [1,L]); 0 skips it")
     ap.add_argument("--lanes", default="4,8,16", help="lane counts the batch autotuner tries")
+    ap.add_argument("--tuning", default="",
+                    help='launch choices as JSON, e.g. {"fuse_ip": 1, "ip_block": 256, '
+                         '"modup_chunk": 24}, instead of autotuning (profiling runs)')
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="length of the open-loop Poisson trace; 0 skips serving")
     ap.add_argument("--serve-rate", type=float, default=1000.0,
@@ -68,11 +71,55 @@ from mkf_b200.replicas import Replicas, dist_env  # noqa: E402
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, ncu, one launch)
 # of the fused decomposition + NTT column pass per source polynomial at
-# logN=16, L1=24, P=4 (C3 top level): one launch over 4 polynomials moved
-# 413.85 MB.  Integer-multiply pipe (sm__pipe_fmaheavy_cycles_active) and
-# issue utilisation from the same capture.
-DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 413.846528e6 / 4}
-DIGITS_COL_PIPES = {(16, 24, 4): {"fmaheavy_cycles_active_pct": 62.3, "issue_active_pct": 52.3}}
+# logN=16, L1=24, P=4 (C3 top level), and the pipe utilisation of the same
+# capture (profiles/digits_col_c3_k2.md).
+DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 407.951104e6 / 4}
+DIGITS_COL_PIPES = {(16, 24, 4): {"fp64_cycles_active_pct": 31.3, "fmaheavy_cycles_active_pct": 29.4,
+                                  "issue_active_pct": 56.1}}
+
+
+def digits_col_compute(L, device, lit, k, L1, nP, kinds):
+    """Compute roofline of the digit column pass: its radix-8 butterflies per
+    second against the ceiling measured on this GPU by mkf_probe_butterflies
+    (a register-resident loop of the transform's own butterflies), float64
+    for moduli below 2^50 and integer for the others.  A product runs the
+    column pass over 2k+1 polynomials (fold of both operands, then the
+    relinearization digit) of beta digits; each digit transforms every limb
+    but its own (level+1+nP limbs, N/2 * n1 butterflies each).  The multSum
+    words rebuilt on the way are extra work, not counted."""
+    if "ntt_digits_col" not in kinds:
+        return None
+    import ctypes
+    peaks = []
+    for kind in (0, 1):
+        v = ctypes.c_double(0.0)
+        if L.mkf_probe_butterflies(device, kind, ctypes.byref(v)) != 0:
+            return None
+        peaks.append(v.value)
+    N, logN = lit.n, lit.log_n
+    n1 = logN - (logN + 1) // 2 if logN > 12 else logN
+    mods = list(lit.q[:L1]) + list(lit.p)
+    beta = (L1 + nP - 1) // nP
+    n_fp = n_int = 0
+    for d in range(beta):
+        own = set(range(d * nP, min((d + 1) * nP, L1)))
+        for li, q in enumerate(mods):
+            if li in own:
+                continue
+            if q < (1 << 50):
+                n_fp += 1
+            else:
+                n_int += 1
+    per_limb = N // 2 * n1
+    polys = 2 * k + 1
+    bfly_fp, bfly_int = polys * n_fp * per_limb, polys * n_int * per_limb
+    ms = kinds["ntt_digits_col"]["ms"] / kinds["ntt_digits_col"]["launches"] * 2
+    achieved = (bfly_fp + bfly_int) / (ms / 1e3) / 1e9
+    peak = (bfly_fp + bfly_int) / (bfly_fp / peaks[1] + bfly_int / peaks[0])
+    return {"unit": "G butterfly/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "peak_int": peaks[0], "peak_fp64": peaks[1], "fp64_share": bfly_fp / (bfly_fp + bfly_int),
+            "peak_source": "mkf_probe_butterflies on this GPU",
+            "counted": "column-pass butterflies per product (2 launches); the fused multSum is extra"}
 
 
 def measured_peaks():
@@ -271,7 +318,12 @@ def run_gpu(a):
         ins.append((l, r))
     # launch choices: time every candidate on this workload, keep the fastest
     from mkf_b200 import autotune
-    tuned = autotune.tune_mkf(P, k, level, operands=(E, ins[0][0], ins[0][1]))
+    if a.tuning:
+        fixed = json.loads(a.tuning)
+        autotune.set_tuning(P, **fixed)
+        tuned = {"best": autotune.get_tuning(P), "ms": {}}
+    else:
+        tuned = autotune.tune_mkf(P, k, level, operands=(E, ins[0][0], ins[0][1]))
     lout = E.output_level(ins[0][0], ins[0][1], True)
     outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(nin)]
     streams = [torch.cuda.Stream() for _ in range(max(1, a.streams))]
@@ -369,8 +421,9 @@ def run_gpu(a):
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
                 "share": tk["ms"] / sum(v["ms"] for v in kinds.values()),
-                "limiter": "integer multiply pipe (IMAD, fmaheavy), not HBM",
-                "int_pipes_ncu": pipes,
+                "limiter": "float64 and integer multiply pipes, not HBM",
+                "pipes_ncu": pipes,
+                "compute": digits_col_compute(L, local, lit, k, L1, nP, kinds),
                 "timed_in": "plain region (one stream, no overlap)"}
 
     # ---- e2e through the C ABI with pinned host buffers -------------------------

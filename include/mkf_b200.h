@@ -406,6 +406,13 @@ mkf_status mkf_profile_read(mkf_ctx *ctx, double *ms, uint64_t *launches, double
  * last reset (instrumentation for the benchmark). */
 uint64_t mkf_launch_count(int reset);
 
+/* Arithmetic ceiling of the NTT passes on `device`: radix-8 butterflies per
+ * second (in units of 1e9) of a register-resident loop with the transform's
+ * own butterflies, kind 0 = integer (moduli below 2^55), kind 1 = float64
+ * (moduli below 2^50).  Takes a few milliseconds; instrumentation for the
+ * benchmark's compute roofline. */
+mkf_status mkf_probe_butterflies(int device, int kind, double *gbfly_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -653,30 +653,26 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
 // Column pass of the NTT of gadget digits with the decomposition fused into
 // its first radix-8 pass.  A block owns C = 2048 / S columns (T = S/8 lanes
 // per column) of one (poly, digit) and walks every target limb:
-// the digit's y_i and float64 corrections for those columns (stored
-// column-major by the prep kernel, coefficient r*2^n2 + cc at cc*2^n1 + r,
-// so the block's columns are contiguous) are staged in shared memory once,
-// and for each limb a multSum word (basis_extension.go:581-646) is rebuilt
-// from them straight into the registers of the first pass.  The transformed
+// for each limb a multSum word (basis_extension.go:581-646) is rebuilt from
+// the digit's y_i and float64 corrections (stored column-major by the prep
+// kernel, coefficient r*2^n2 + cc at cc*2^n1 + r, so that a column's words
+// are contiguous; they stay in L2 across the limbs) straight into the
+// registers of the first pass.  The transformed
 // columns are stored row-major through the exchange tile, for the row pass.
 // One-limb digits are reduced from the coefficient-domain source limb (staged
 // once); own limbs are copied from the NTT-domain input (src.own) or, without
 // one, reduced from the source limb.  The integer multSum's 128-bit sum needs
 // no reduction on the way: its high word stays below ns * q_i * p_j / 2^64.
 constexpr int kColThreads = 256, kColWords = 2048;
-// dynamic shared memory for alpha staged limbs (alpha <= 8: 146 KB); the
-// kernel's attribute is set once for alpha = 8
-inline size_t digits_col_smem(int alpha) {
-    return (size_t)kColWords * 8 * (1 + std::max(alpha, 1)) + kColWords;
-}
+// dynamic shared memory: the exchange tile and one staged source limb
+constexpr size_t kColSmem = (size_t)kColWords * 8 * 2;
 
 template <int LOGS>
-__global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
+__global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kColWords / S, NW = kColWords;
     extern __shared__ __align__(16) uint64_t dsm[];
     uint64_t *s = dsm;                 // exchange tile, C columns
-    uint64_t *ys = dsm + NW;           // [alpha][C][S] staged y_i (or the one-limb source)
-    uint8_t *vs = reinterpret_cast<uint8_t *>(ys + (size_t)NW * max(src.alpha, 1));
+    uint64_t *ys = dsm + NW;           // [C][S] the staged one-limb source
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y, poly = pd / src.ndigits, d = pd % src.ndigits;
     const int N = 1 << a.logN, R = 1 << a.n2;
@@ -686,16 +682,9 @@ __global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, 
     const bool msum = ns >= 2 && src.tabs;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
     const int col0 = blockIdx.x * C;
-    // stage the digit's sources for the block's columns
-    if (msum) {
-        const ulonglong2 *yg = reinterpret_cast<const ulonglong2 *>(src.y + (long long)pd * src.alpha * N +
-                                                                   (long long)col0 * S);
-        for (int i = 0; i < ns; ++i)
-            for (int e = tid; e < NW / 2; e += kColThreads)
-                reinterpret_cast<ulonglong2 *>(ys + (size_t)i * NW)[e] = __ldg(yg + (size_t)i * N / 2 + e);
-        const uint4 *vg = reinterpret_cast<const uint4 *>(src.v + (long long)pd * N + (long long)col0 * S);
-        for (int e = tid; e < NW / 16; e += kColThreads) reinterpret_cast<uint4 *>(vs)[e] = __ldg(vg + e);
-    } else if (ns == 1) {
+    // a one-limb digit's source limb is staged for the block's columns; the
+    // y_i of a multSum digit are read from L2 for every limb
+    if (!msum && ns == 1) {
         const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)start * N;
         for (int idx = tid; idx < NW; idx += kColThreads) {
             const int r = idx / C, cc = idx % C;
@@ -753,8 +742,8 @@ __global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, 
         } else {
             const int row = l < L1 ? l : src.nQ + (l - L1);
             const uint64_t *tvr = tb->vq + row * (ns + 1);
-            const uint64_t *yl = ys + c * S + t;
-            const uint8_t *vl = vs + c * S + t;
+            const uint64_t *yl = src.y + (long long)pd * src.alpha * N + (long long)(col0 + c) * S + t;
+            const uint8_t *vl = src.v + (long long)pd * N + (long long)(col0 + c) * S + t;
             if (fp && tb->fp_src) {
                 // float64 multSum: each y_i * (Q/q_i mod p) reduced by
                 // mulmod_f (|.| <= 5p/8), the terms and the correction
@@ -767,12 +756,12 @@ __global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, 
                     const double cq = __ldg(tb->qmodd + (row * ns + i) * 2 + 1);
 #pragma unroll
                     for (int r = 0; r < 8; ++r)
-                        acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(yl[i * NW + r * T]), cw, cq, md.qd));
+                        acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(__ldg(yl + (long long)i * N + r * T)), cw, cq, md.qd));
                 }
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
                     vi[r] = (uint64_t)__double_as_longlong(
-                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + vl[r * T]))), md.qinvd, md.qd));
+                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + __ldg(vl + r * T)))), md.qinvd, md.qd));
             } else {
                 // integer multSum, four words at a time
 #pragma unroll
@@ -783,12 +772,12 @@ __global__ void __launch_bounds__(kColThreads, 2) ntt_fwd_digits_col(NttArgs a, 
                     for (int i = 0; i < ns; ++i) {
                         const uint64_t b = __ldg(tb->qmod + row * ns + i);
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], yl[i * NW + (h + r) * T], b);
+                        for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], __ldg(yl + (long long)i * N + (h + r) * T), b);
                     }
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
                         const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
-                        const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + vl[(h + r) * T]), q);
+                        const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + __ldg(vl + (h + r) * T)), q);
                         vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
                     }
                 }
@@ -1181,8 +1170,8 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             sb.own_out = b.ls.base;                                                                \
             dim3 g1((1 << L2G) / (kColWords >> L1G), npp);                                         \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
-            smem_attr(ntt_fwd_digits_col<L1G>, c.device, digits_col_smem(8));                  \
-            ntt_fwd_digits_col<L1G><<<g1, kColThreads, digits_col_smem(src.alpha), st>>>(b, sb);   \
+            smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
+            ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
             if (p0) note_launch(1);                                                                \
         }                                                                                          \
         dim3 g2((1 << L1G) / (kTile >> L2G), limbs, ip.groups * ip.nin);                           \
@@ -1208,9 +1197,9 @@ void ntt_prepare(const Context &c) {
     smem_attr(ntt_fwd_phase<7, false>, c.device, fwd_phase_smem<7, false>());
     smem_attr(ntt_fwd_phase<8, false>, c.device, fwd_phase_smem<8, false>());
     smem_attr(ntt_digits_row_ip<7>, c.device, kRowIpSmem);
-    smem_attr(ntt_fwd_digits_col<6>, c.device, digits_col_smem(8));
-    smem_attr(ntt_fwd_digits_col<7>, c.device, digits_col_smem(8));
-    smem_attr(ntt_fwd_digits_col<8>, c.device, digits_col_smem(8));
+    smem_attr(ntt_fwd_digits_col<6>, c.device, kColSmem);
+    smem_attr(ntt_fwd_digits_col<7>, c.device, kColSmem);
+    smem_attr(ntt_fwd_digits_col<8>, c.device, kColSmem);
     smem_attr(ntt_digits_row_ip<8>, c.device, kRowIpSmem);
 }
 
@@ -1262,8 +1251,8 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         dim3 g1((1 << L2G) / (kColWords >> L1G), npp), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
-            smem_attr(ntt_fwd_digits_col<L1G>, c.device, digits_col_smem(8));                  \
-            ntt_fwd_digits_col<L1G><<<g1, kColThreads, digits_col_smem(src.alpha), st>>>(b, sb);   \
+            smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
+            ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \
