@@ -36,6 +36,7 @@ struct DevModulus {
     double qinvd;     // 1/q rounded to double
     double ninvd, ninvq; // ninv and ninv/q as doubles (float64 inverse NTT)
     double lastd, lastq; // last and last/q as doubles
+    double r64d, r64q;   // 2^-64 mod q, centered, and that / q (float64 MRed)
 };
 
 // A twiddle with its Shoup companion, loaded as one 16-byte word.
@@ -142,11 +143,19 @@ constexpr uint64_t kFp64Bound = 1ull << 50;
 // v*w - k*q with k = round(v*w/q): h + l = v*w exactly (two-product), k from
 // wq = w/q (relative error 2^-53) is within 1/2 + |v|*2^-53 of v*w/q, and
 // h - k*q and its sum with l are integers below 2^53, hence exact.  Needs
-// |v| < 2^51; returns |r| <= (1/2 + |v|*2^-53) * q.
+// |v * w/q| < 2^51; returns |r| <= (1/2 + |v * w/q| * 2^-53) * q.
 MKF_DEV double mulmod_f(double v, double w, double wq, double q) {
     const double h = __dmul_rn(v, w);
     const double l = __fma_rn(v, w, -h);
     const double k = __dadd_rn(__fma_rn(v, wq, MKF_F_RND), -MKF_F_RND);
+    return __dadd_rn(__fma_rn(-k, q, h), l);
+}
+// a*b - k*q for two variable words, k = round(h/q) from the rounded product
+// h: exact while |a*b| <= 2^51 q, |result| <= (1/2 + |a*b|/(q 2^52)) q.
+MKF_DEV double mulvar_f(double a, double b, double q, double qinv) {
+    const double h = __dmul_rn(a, b);
+    const double l = __fma_rn(a, b, -h);
+    const double k = __dadd_rn(__fma_rn(h, qinv, MKF_F_RND), -MKF_F_RND);
     return __dadd_rn(__fma_rn(-k, q, h), l);
 }
 // x - round(x/q)*q, |result| <= q/2 (plus a rounding unit of the quotient).

@@ -333,6 +333,12 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         d.ninvq = (double)d.ninv / (double)qq;
         d.lastd = (double)d.last;
         d.lastq = (double)d.last / (double)qq;
+        {
+            const uint64_t r64 = h_invmod(d.mont1, qq);
+            const long long rc = r64 > qq / 2 ? (long long)r64 - (long long)qq : (long long)r64;
+            d.r64d = (double)rc;
+            d.r64q = (double)rc / (double)qq;
+        }
         for (int k = 0; k < S1; ++k) {
             fwd1[(size_t)m * S1 + k] = Tw{rev[k], h_shoup(rev[k], qq)};
             inv1[(size_t)m * S1 + k] = Tw{irev[k], h_shoup(irev[k], qq)};

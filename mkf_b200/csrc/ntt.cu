@@ -1061,37 +1061,72 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N + rowoff + t;
     const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
     const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-    for (int d = 0; d < g.beta; ++d) {
-        const int start = d * g.alpha;
-        const bool own = g.own.p[0] && l < g.L1 && l >= start &&
-                         l < start + digit_ns(g.level, g.alpha, d);
-        uint64_t v[8];
-        if (own) {
-            const uint64_t *xn = (poly < g.own.split
-                                      ? g.own.p[0] + (long long)poly * g.own.pstride[0]
-                                      : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
-                                 (long long)l * N + rowoff + t;
+    if (fp) {
+        // float64 limbs: the products with the keys (Montgomery forms) are
+        // formed by mulvar_f on centered words and summed as doubles; the
+        // sum times 2^-64 is MRed's sum.  Bounds (q < 2^50): NTT outputs
+        // below 3.6q, keys below q/2, each product below 0.95q, the sums
+        // below 0.5q + 4 * 0.95q.
+        double *f0 = reinterpret_cast<double *>(acc0), *f1 = reinterpret_cast<double *>(acc1);
+        for (int d = 0; d < g.beta; ++d) {
+            const int start = d * g.alpha;
+            const bool own = g.own.p[0] && l < g.L1 && l >= start &&
+                             l < start + digit_ns(g.level, g.alpha, d);
+            double v[8];
+            if (own) {
+                const uint64_t *xn = (poly < g.own.split
+                                          ? g.own.p[0] + (long long)poly * g.own.pstride[0]
+                                          : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
+                                     (long long)l * N + rowoff + t;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = xn[k * T];
-        } else {
-            // the first radix-8 pass holds points r*T + t: load them directly
-            const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N + rowoff + t;
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = src[r * T];
-            if (fp) {
-                double vf[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
-                // words below 4q: x + 4q is a non-negative integer below 2^53,
-                // which MRed takes as it is
-                fwd_passes_f<LOGS, 32, 64, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
-                const double off = 4.0 * md.qd + MKF_F_2P52;
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    v[k] = (uint64_t)__double_as_longlong(
-                               __dadd_rn(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), off)) -
-                           0x4330000000000000ull;
+                for (int k = 0; k < 8; ++k) v[k] = centered_f(xn[k * T], q);
             } else {
+                const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N + rowoff + t;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)src[r * T]);
+                fwd_passes_f<LOGS, 32, 64, false, false, true>(s, twd, md.qd, md.qinvd, c, t, v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = __longlong_as_double((long long)s[saddr<S>(c, k * T + t)]);
+            }
+            const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
+            const uint64_t *k1 = k0 + g.k_ostride;
+            // every fourth digit the sums go back to q/2 (more digits than six)
+            const bool red = (d & 3) == 3;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                double x0 = __dadd_rn(f0[k * T], mulvar_f(v[k], centered_f(__ldg(k0 + k * T), q), md.qd, md.qinvd));
+                double x1 = __dadd_rn(f1[k * T], mulvar_f(v[k], centered_f(__ldg(k1 + k * T), q), md.qd, md.qinvd));
+                if (red) {
+                    x0 = reduce_f(x0, md.qinvd, md.qd);
+                    x1 = reduce_f(x1, md.qinvd, md.qd);
+                }
+                f0[k * T] = x0;
+                f1[k * T] = x1;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            acc0[k * T] = canon_f(mulmod_f(reduce_f(f0[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
+            acc1[k * T] = canon_f(mulmod_f(reduce_f(f1[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
+        }
+    } else {
+        for (int d = 0; d < g.beta; ++d) {
+            const int start = d * g.alpha;
+            const bool own = g.own.p[0] && l < g.L1 && l >= start &&
+                             l < start + digit_ns(g.level, g.alpha, d);
+            uint64_t v[8];
+            if (own) {
+                const uint64_t *xn = (poly < g.own.split
+                                          ? g.own.p[0] + (long long)poly * g.own.pstride[0]
+                                          : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
+                                     (long long)l * N + rowoff + t;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = xn[k * T];
+            } else {
+                // the first radix-8 pass holds points r*T + t: load them directly
+                const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N + rowoff + t;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[r] = src[r * T];
                 if (lazy)
                     fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
                 else
@@ -1099,13 +1134,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
 #pragma unroll
                 for (int k = 0; k < 8; ++k) v[k] = s[saddr<S>(c, k * T + t)];
             }
-        }
-        const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
-        const uint64_t *k1 = k0 + g.k_ostride;
+            const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
+            const uint64_t *k1 = k0 + g.k_ostride;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            acc0[k * T] = add_mod(acc0[k * T], mred(v[k], __ldg(k0 + k * T), q, md.qinv), q);
-            acc1[k * T] = add_mod(acc1[k * T], mred(v[k], __ldg(k1 + k * T), q, md.qinv), q);
+            for (int k = 0; k < 8; ++k) {
+                acc0[k * T] = add_mod(acc0[k * T], mred(v[k], __ldg(k0 + k * T), q, md.qinv), q);
+                acc1[k * T] = add_mod(acc1[k * T], mred(v[k], __ldg(k1 + k * T), q, md.qinv), q);
+            }
         }
     }
     uint64_t *o0 = g.out + (long long)grp * g.out_gstride + (long long)sidx * g.out_istride +
