@@ -34,8 +34,8 @@ struct DevModulus {
     double qd;        // (double)q, as the reference's float64 correction uses
     uint64_t one_sh;  // floor(2^64 / q): Shoup companion of 1
     double qinvd;     // 1/q rounded to double
-    double ninvd, ninvq; // ninv and ninv/q as doubles (float64 inverse NTT)
-    double lastd, lastq; // last and last/q as doubles
+    double ninvd, ninvq; // ninv centered and that / q (float64 inverse NTT)
+    double lastd, lastq; // last centered and that / q
     double r64d, r64q;   // 2^-64 mod q, centered, and that / q (float64 MRed)
 };
 

@@ -329,10 +329,15 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
         }
         d.last = h_mulmod(irev[1], d.ninv, qq);
         d.last_sh = h_shoup(d.last, qq);
-        d.ninvd = (double)d.ninv;
-        d.ninvq = (double)d.ninv / (double)qq;
-        d.lastd = (double)d.last;
-        d.lastq = (double)d.last / (double)qq;
+        {
+            // centered, as the float64 twiddles
+            const long long nc = d.ninv > qq / 2 ? (long long)d.ninv - (long long)qq : (long long)d.ninv;
+            const long long lc = d.last > qq / 2 ? (long long)d.last - (long long)qq : (long long)d.last;
+            d.ninvd = (double)nc;
+            d.ninvq = (double)nc / (double)qq;
+            d.lastd = (double)lc;
+            d.lastq = (double)lc / (double)qq;
+        }
         {
             const uint64_t r64 = h_invmod(d.mont1, qq);
             const long long rc = r64 > qq / 2 ? (long long)r64 - (long long)qq : (long long)r64;

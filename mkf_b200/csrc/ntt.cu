@@ -95,15 +95,43 @@ __device__ __forceinline__ void ct_bfly_f(double &U, double &V, const TwD w, dou
     V = __dadd_rn(u, -t);
 }
 
-// Float64 Gentleman-Sande butterfly: U' = U + V reduced to |U'| <= q/2 and
-// V' = (U - V) w.  From |U|, |V| <= B q with B <= 1 (|U - V| < 2q, the
-// rounding trick's range) V' stays below (1/2 + B/4) q, so the bound settles
-// near 2q/3 and every stage keeps it.
+// Float64 Gentleman-Sande butterfly: U' = U + V, reduced to |U'| <= q/2 when
+// RED, and V' = (U - V) w.  With centered twiddles and |U|, |V| <= B q,
+// |U - V| <= 2B q must stay below 3.9q (the rounding trick's range, q < 2^50);
+// then V' <= (1/2 + B/8) q and U' <= 2B q (or q/2).  gsched below picks the
+// stages that reduce.
+template <bool RED>
 __device__ __forceinline__ void gs_bfly_f(double &U, double &V, const TwD w, double q, double qi) {
-    const double x = reduce_f(__dadd_rn(U, V), qi, q);
+    const double s = __dadd_rn(U, V);
     V = mulmod_f(__dadd_rn(U, -V), w.w, w.wq, q);
-    U = x;
+    U = RED ? reduce_f(s, qi, q) : s;
 }
+
+// Greedy reduction schedule of the float64 inverse passes (bounds in units of
+// q, as above): stage st (run from LOGS-1 down to 0) reduces U' when the next
+// stage could not run from the unreduced bound, or, at the last stage of a
+// row phase, when the output would exceed OUT16/16.  A column phase's stage 0
+// is the N^-1 stage (both outputs through mulmod_f).  Bit st of the mask.
+namespace gsched {
+constexpr double kV = 3.9, kEps = 1.0 / 1024;
+constexpr unsigned mask(int LOGS, int in16, bool cols, int out16) {
+    double b = in16 / 16.0;
+    unsigned m = 0;
+    for (int st = LOGS - 1; st >= 0; --st) {
+        if (2 * b > kV) return ~0u; // input bound too large: reduce everywhere
+        if (cols && st == 0) break;
+        const double nr = 2 * b > 0.5 + b / 8 + kEps ? 2 * b : 0.5 + b / 8 + kEps;
+        const bool red = st > 0 ? 2 * nr > kV : nr > out16 / 16.0;
+        if (red) {
+            m |= 1u << st;
+            b = 0.5 + b / 8 + kEps;
+        } else {
+            b = nr;
+        }
+    }
+    return m;
+}
+} // namespace gsched
 
 // MODE 0: whole limb in one tile. MODE 1: column pass. MODE 2: row pass.
 template <int MODE>
@@ -666,6 +694,8 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
 constexpr int kColThreads = 256, kColWords = 2048;
 // dynamic shared memory: the exchange tile and one staged source limb
 constexpr size_t kColSmem = (size_t)kColWords * 8 * 2;
+// blocks per (poly, digit, column tile), each walking a share of the limbs
+constexpr int kColLimbSplit = 4;
 
 template <int LOGS>
 __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
@@ -693,7 +723,11 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
     }
     __syncthreads();
     const ModUpTab *tb = msum ? src.tabs + d * (src.alpha + 1) + ns : nullptr;
-    for (int l = 0; l < limbs; ++l) {
+    // this block's share of the limbs (grid.z splits them, against the tail
+    // of the last wave)
+    const int per = (limbs + gridDim.z - 1) / gridDim.z;
+    const int l_end = min(limbs, (int)(blockIdx.z + 1) * per);
+    for (int l = blockIdx.z * per; l < l_end; ++l) {
         const bool own_limb = l < L1 && l >= start && l < start + ns;
         uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
         if (own_limb && src.own.p[0]) {
@@ -851,9 +885,14 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
 // The passes of an inverse phase in float64 (limbs below 2^50), on the bits
 // of centered doubles; COLS: the last phase, whose global stage 0 folds in
 // N^-1 (both outputs then below 2q/3).
+// Row phases take centered words (IN 1/2) and hand the column phase words
+// below 1.375q.
+constexpr int kInvRowIn16 = 8, kInvMid16 = 22;
 template <int LOGS, bool COLS>
 MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int c, int t) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    constexpr unsigned RED = COLS ? gsched::mask(LOGS, kInvMid16, true, 0)
+                                  : gsched::mask(LOGS, kInvRowIn16, false, kInvMid16);
     const double q = md.qd, qi = md.qinvd;
     double v[8];
 #pragma unroll
@@ -874,7 +913,10 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
                         V = mulmod_f(__dadd_rn(U, -V), md.lastd, md.lastq, q);
                         U = x;
                     } else {
-                        gs_bfly_f(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
+                        if ((RED >> st) & 1)
+                            gs_bfly_f<true>(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
+                        else
+                            gs_bfly_f<false>(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
                     }
                 }
             }
@@ -1203,7 +1245,7 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             sb.v = src.v + (long long)p0 * c.N;                                                    \
             sb.poly0 = first_poly;                                                                 \
             sb.own_out = b.ls.base;                                                                \
-            dim3 g1((1 << L2G) / (kColWords >> L1G), npp);                                         \
+            dim3 g1((1 << L2G) / (kColWords >> L1G), npp, kColLimbSplit);                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
             ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
@@ -1283,7 +1325,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         switch (c.logN) {
 #define MKF_DIGITS_CASE(LN, L1G, L2G)                                                              \
     case LN: {                                                                                     \
-        dim3 g1((1 << L2G) / (kColWords >> L1G), npp), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
+        dim3 g1((1 << L2G) / (kColWords >> L1G), npp, kColLimbSplit), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
