@@ -72,10 +72,10 @@ from mkf_b200.replicas import Replicas, dist_env  # noqa: E402
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, ncu, one launch)
 # of the fused decomposition + NTT column pass per source polynomial at
 # logN=16, L1=24, P=4 (C3 top level), and the pipe utilisation of the same
-# capture (profiles/digits_col_c3_k2.md).
-DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 407.951104e6 / 4}
-DIGITS_COL_PIPES = {(16, 24, 4): {"fp64_cycles_active_pct": 31.3, "fmaheavy_cycles_active_pct": 29.4,
-                                  "issue_active_pct": 56.1}}
+# capture (profiles/digits_col_row_ip_c3_k2.md): 388.8 MB over 4 polynomials.
+DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 388.813e6 / 4}
+DIGITS_COL_PIPES = {(16, 24, 4): {"fp64_cycles_active_pct": 34.3, "fmaheavy_cycles_active_pct": 33.3,
+                                  "issue_active_pct": 60.6}}
 
 
 def digits_col_compute(L, device, lit, k, L1, nP, kinds):
