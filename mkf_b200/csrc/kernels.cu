@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
                                                              const DevModulus *mods, uint64_t *y,
                                                              uint8_t *v, int level, int alpha,
                                                              int ndigits, int N, int n1, int n2) {
-    __shared__ uint64_t tile[32][33];
+    __shared__ uint64_t tile[2][32][33]; // double-buffered: one barrier per limb
     __shared__ uint8_t vt[32][33];
     const int d = blockIdx.y, p = blockIdx.z;
     const int ns = (level > alpha * (d + 1) - 1 ? alpha - 2 : (level % alpha) - 1) + 2;
@@ -125,24 +125,36 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
     const uint64_t *xp = in + (long long)p * in_pstride + (long long)d * alpha * N;
     const long long pd = (long long)p * ndigits + d;
     uint64_t *yp = y + pd * alpha * N;
+    // every source word of the tile is loaded before any is used (at most
+    // 8 limbs: alpha <= 8)
+    uint64_t xs[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < ns) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                xs[i][k] = xp[(long long)i * N + ((long long)(r0 + ty + 8 * k) << n2) + c0 + tx];
+        }
     double vi[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = 0; i < ns; ++i) {
-        const DevModulus &m = mods[tab.src_mod[i]];
-        const uint64_t inv = tab.inv[i];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int rr = ty + 8 * k;
-            const uint64_t yi = mred(xp[(long long)i * N + ((long long)(r0 + rr) << n2) + c0 + tx], inv, m.q, m.qinv);
-            vi[k] = __dadd_rn(vi[k], __ddiv_rn(__ull2double_rn(yi), m.qd));
-            tile[rr][tx] = yi;
-        }
-        __syncthreads();
+    for (int i = 0; i < 8; ++i) {
+        if (i < ns) {
+            const DevModulus &m = mods[tab.src_mod[i]];
+            const uint64_t inv = tab.inv[i];
+            uint64_t(*tl)[33] = tile[i & 1];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int cj = ty + 8 * k;
-            yp[(long long)i * N + ((long long)(c0 + cj) << n1) + r0 + tx] = tile[tx][cj];
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t yi = mred(xs[i][k], inv, m.q, m.qinv);
+                vi[k] = __dadd_rn(vi[k], __ddiv_rn(__ull2double_rn(yi), m.qd));
+                tl[ty + 8 * k][tx] = yi;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int cj = ty + 8 * k;
+                yp[(long long)i * N + ((long long)(c0 + cj) << n1) + r0 + tx] = tl[tx][cj];
+            }
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) vt[ty + 8 * k][tx] = (uint8_t)__double2ull_rz(vi[k]);
