@@ -371,20 +371,31 @@ def run_gpu(a):
     L.mkf_profile_enable(P.handle, 0)
 
     # ---- batched: `batch` products per step over `streams` streams -------------
-    def batched_step(step):
+    # Steps are pipelined: stream j%streams issues product j of every step in
+    # order (reusing its own operands and outputs), so a step's products start
+    # as soon as their stream is free instead of waiting for the whole
+    # previous step; the streams fork from and join into streams[0] around the
+    # timed region only.
+    def fork():
         start = torch.cuda.Event()
         start.record(streams[0])
         for s in streams[1:]:
             s.wait_event(start)
-        for j in range(a.batch):
-            product(step * a.batch + j, streams[j % len(streams)])
+
+    def join():
         for s in streams[1:]:
             e = torch.cuda.Event()
             e.record(s)
             streams[0].wait_event(e)
 
+    def batched_step(step):
+        for j in range(a.batch):
+            product(step * a.batch + j, streams[j % len(streams)])
+
+    fork()
     for i in range(a.warmup):
         batched_step(i)
+    join()
     barrier()
     L.mkf_launch_count(1)
     clocks = ClockSampler(local)
@@ -393,8 +404,10 @@ def run_gpu(a):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(streams[0])
+    fork()
     for step in range(a.steps):
         batched_step(step)
+    join()
     t1.record(streams[0])
     t1.synchronize()
     barrier()
@@ -445,10 +458,6 @@ def run_gpu(a):
         e_outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.batch)]
 
         def e2e_step():
-            start = torch.cuda.Event()
-            start.record(streams[0])
-            for s in streams[1:]:
-                s.wait_event(start)
             for j in range(a.batch):
                 s = streams[j % len(streams)]
                 cs = ctypes_stream(s)
@@ -460,17 +469,18 @@ def run_gpu(a):
                 E.MulRelin(l, r, e_outs[j], rescale=True, materialize=True, stream=cs)
                 capi.check(P.handle, L.mkf_ct_download_async(
                     e_outs[j].handle, ctypes.cast(hout[j].data_ptr(), capi.u64p), words_out, cs))
-            for s in streams[1:]:
-                e = torch.cuda.Event()
-                e.record(s)
-                streams[0].wait_event(e)
 
+        fork()
         for _ in range(a.warmup):
             e2e_step()
+        join()
+        torch.cuda.synchronize()
         barrier()
         t0.record(streams[0])
+        fork()
         for _ in range(a.steps):
             e2e_step()
+        join()
         t1.record(streams[0])
         t1.synchronize()
         barrier()
@@ -507,23 +517,20 @@ def run_gpu(a):
         barrier()
 
         def batched8(step):
-            start = torch.cuda.Event()
-            start.record(streams[0])
-            for s in streams[1:]:
-                s.wait_event(start)
             for j in range(a.batch):
                 product8(step * a.batch + j, streams[j % len(streams)])
-            for s in streams[1:]:
-                e = torch.cuda.Event()
-                e.record(s)
-                streams[0].wait_event(e)
 
+        fork()
         for i in range(a.warmup):
             batched8(i)
+        join()
+        torch.cuda.synchronize()
         barrier()
         t0.record(streams[0])
+        fork()
         for step in range(a.steps):
             batched8(step)
+        join()
         t1.record(streams[0])
         t1.synchronize()
         barrier()

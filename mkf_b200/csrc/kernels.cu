@@ -486,7 +486,8 @@ __global__ void __launch_bounds__(kBlock) moddown_combine_kernel(CombineSpec a, 
     uint64_t r = 0;
     if (a.y_single) {
         uint64_t xs = 0;
-        for (int t = 0; t < a.terms; ++t) xs = add_mod(xs, a.x[xo + (long long)t * a.x_tstride], m.q);
+#pragma unroll 8
+        for (int t = 0; t < a.terms; ++t) xs = add_mod(xs, __ldg(a.x + xo + (long long)t * a.x_tstride), m.q);
         r = mred(a.y[yo] + 2 * m.q - xs, c, m.q, m.qinv);
     } else
     for (int t = 0; t < a.terms; ++t) {
