@@ -723,6 +723,14 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
     }
     __syncthreads();
     const ModUpTab *tb = msum ? src.tabs + d * (src.alpha + 1) + ns : nullptr;
+    // the float64 corrections of this thread's 8 first-pass words are the
+    // same for every target limb: loaded once, one byte each
+    uint32_t vpk[2] = {0u, 0u};
+    if (msum) {
+        const uint8_t *vl = src.v + (long long)pd * N + (long long)(col0 + c) * S + t;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) vpk[r >> 2] |= (uint32_t)__ldg(vl + r * T) << (8 * (r & 3));
+    }
     // this block's share of the limbs (grid.z splits them, against the tail
     // of the last wave)
     const int per = (limbs + gridDim.z - 1) / gridDim.z;
@@ -777,7 +785,6 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             const int row = l < L1 ? l : src.nQ + (l - L1);
             const uint64_t *tvr = tb->vq + row * (ns + 1);
             const uint64_t *yl = src.y + (long long)pd * src.alpha * N + (long long)(col0 + c) * S + t;
-            const uint8_t *vl = src.v + (long long)pd * N + (long long)(col0 + c) * S + t;
             if (fp && tb->fp_src) {
                 // float64 multSum: each y_i * (Q/q_i mod p) reduced by
                 // mulmod_f (|.| <= 5p/8), the terms and the correction
@@ -795,7 +802,8 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
                     vi[r] = (uint64_t)__double_as_longlong(
-                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + __ldg(vl + r * T)))), md.qinvd, md.qd));
+                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + ((vpk[r >> 2] >> (8 * (r & 3))) & 0xffu)))),
+                                 md.qinvd, md.qd));
             } else {
                 // integer multSum, four words at a time
 #pragma unroll
@@ -811,7 +819,8 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
                         const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
-                        const uint64_t x = canon3(hi[r] - hh + q + __ldg(tvr + __ldg(vl + (h + r) * T)), q);
+                        const uint64_t x = canon3(
+                            hi[r] - hh + q + __ldg(tvr + ((vpk[(h + r) >> 2] >> (8 * ((h + r) & 3))) & 0xffu)), q);
                         vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
                     }
                 }
