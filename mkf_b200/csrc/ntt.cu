@@ -133,192 +133,63 @@ constexpr unsigned mask(int LOGS, int in16, bool cols, int out16) {
 }
 } // namespace gsched
 
-// MODE 0: whole limb in one tile. MODE 1: column pass. MODE 2: row pass.
-template <int MODE>
-__global__ void __launch_bounds__(kThreads) ntt_fwd_kernel(NttArgs a) {
+// logN <= 12: a whole limb of N <= 4096 words in one tile, one stage per
+// barrier (Harvey butterflies; outputs canonical).
+__global__ void __launch_bounds__(kThreads) ntt_fwd_tile(NttArgs a) {
     __shared__ uint64_t s[kTile];
-    const int limb_total = a.ls.limbs;
-    const int poly = blockIdx.y / limb_total, l = blockIdx.y % limb_total;
+    const int poly = blockIdx.y / a.ls.limbs, l = blockIdx.y % a.ls.limbs;
     const int m = a.ls.mod_of(l);
     const uint64_t q = a.mods[m].q;
     const int N = 1 << a.logN;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x;
-
-    int S, C, nst;
-    if (MODE == 0) {
-        S = N;
-        C = 1;
-        nst = a.logN;
-    } else if (MODE == 1) {
-        S = 1 << a.n1;
-        C = kTile / S;
-        nst = a.n1;
-    } else {
-        S = 1 << a.n2;
-        C = kTile / S;
-        nst = a.n2;
-    }
-    const int R = 1 << a.n2; // row length (MODE 1)
-    const int total = S * C;
-    // load
-    if (MODE == 1) {
-        const int c0 = blockIdx.x * C;
-        for (int idx = tid; idx < total; idx += kThreads) {
-            int r = idx / C, cc = idx - r * C;
-            s[idx] = data[(long long)r * R + c0 + cc];
-        }
-    } else {
-        const long long off = (long long)blockIdx.x * total;
-        for (int idx = tid; idx < total; idx += kThreads) s[idx] = data[off + idx];
-    }
+    for (int idx = tid; idx < N; idx += kThreads) s[idx] = data[idx];
     __syncthreads();
-    const Tw *tw1 = a.tw1 + (size_t)m * (1 << a.n1);
-    const Tw *tw2 = a.tw2 ? a.tw2 + (size_t)m * N : nullptr;
-    const int half = total / 2;
-    for (int st = 0; st < nst; ++st) {
-        const int t = S >> (st + 1);
-        for (int b = tid; b < half; b += kThreads) {
-            int e, cc = 0, rr = 0, i;
-            if (MODE == 1) {
-                cc = b % C;
-                int p = b / C;
-                i = p / t;
-                int j = p - i * t;
-                int r = 2 * i * t + j;
-                e = r * C + cc;
-                uint64_t U = s[e], V = s[e + t * C];
-                ct_bfly(U, V, tw1[(1 << st) + i], q);
-                s[e] = U;
-                s[e + t * C] = V;
-            } else {
-                int hs = S / 2;
-                rr = b / hs;
-                int p = b - rr * hs;
-                i = p / t;
-                int j = p - i * t;
-                e = rr * S + 2 * i * t + j;
-                Tw w;
-                if (MODE == 0)
-                    w = tw1[(1 << st) + i];
-                else
-                    w = tw2[(size_t)(blockIdx.x * C + rr) * S + (1 << st) + i];
-                uint64_t U = s[e], V = s[e + t];
-                ct_bfly(U, V, w, q);
-                s[e] = U;
-                s[e + t] = V;
-            }
+    const Tw *tw = a.tw1 + (size_t)m * N;
+    for (int st = 0; st < a.logN; ++st) {
+        const int t = N >> (st + 1);
+        for (int b = tid; b < N / 2; b += kThreads) {
+            const int i = b / t, e = 2 * i * t + (b - i * t);
+            uint64_t U = s[e], V = s[e + t];
+            ct_bfly(U, V, tw[(1 << st) + i], q);
+            s[e] = U;
+            s[e + t] = V;
         }
         __syncthreads();
     }
-    // store
-    if (MODE == 1) {
-        const int c0 = blockIdx.x * C;
-        for (int idx = tid; idx < total; idx += kThreads) {
-            int r = idx / C, cc = idx - r * C;
-            data[(long long)r * R + c0 + cc] = s[idx];
-        }
-    } else {
-        const long long off = (long long)blockIdx.x * total;
-        for (int idx = tid; idx < total; idx += kThreads) data[off + idx] = reduce4(s[idx], q);
-    }
+    for (int idx = tid; idx < N; idx += kThreads) data[idx] = reduce4(s[idx], q);
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads) ntt_inv_kernel(NttArgs a) {
+__global__ void __launch_bounds__(kThreads) ntt_inv_tile(NttArgs a) {
     __shared__ uint64_t s[kTile];
-    const int limb_total = a.ls.limbs;
-    const int poly = blockIdx.y / limb_total, l = blockIdx.y % limb_total;
+    const int poly = blockIdx.y / a.ls.limbs, l = blockIdx.y % a.ls.limbs;
     const int m = a.ls.mod_of(l);
     const DevModulus md = a.mods[m];
     const uint64_t q = md.q;
     const int N = 1 << a.logN;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x;
-
-    int S, C, nst;
-    if (MODE == 0) {
-        S = N;
-        C = 1;
-        nst = a.logN;
-    } else if (MODE == 1) {
-        S = 1 << a.n1;
-        C = kTile / S;
-        nst = a.n1;
-    } else {
-        S = 1 << a.n2;
-        C = kTile / S;
-        nst = a.n2;
-    }
-    const int R = 1 << a.n2;
-    const int total = S * C;
-    if (MODE == 1) {
-        const int c0 = blockIdx.x * C;
-        for (int idx = tid; idx < total; idx += kThreads) {
-            int r = idx / C, cc = idx - r * C;
-            s[idx] = data[(long long)r * R + c0 + cc];
-        }
-    } else {
-        const long long off = (long long)blockIdx.x * total;
-        for (int idx = tid; idx < total; idx += kThreads) s[idx] = data[off + idx];
-    }
+    for (int idx = tid; idx < N; idx += kThreads) s[idx] = data[idx];
     __syncthreads();
-    const Tw *tw1 = a.tw1 + (size_t)m * (1 << a.n1);
-    const Tw *tw2 = a.tw2 ? a.tw2 + (size_t)m * N : nullptr;
-    const int half = total / 2;
-    const bool has_last = (MODE != 2); // global stage 0 lives in this pass
-    for (int st = nst - 1; st >= 0; --st) {
-        const int t = S >> (st + 1);
-        const bool last = has_last && st == 0;
-        for (int b = tid; b < half; b += kThreads) {
-            int e, stride, i;
-            Tw w;
-            if (MODE == 1) {
-                int cc = b % C;
-                int p = b / C;
-                i = p / t;
-                int j = p - i * t;
-                int r = 2 * i * t + j;
-                e = r * C + cc;
-                stride = t * C;
-                w = tw1[(1 << st) + i];
+    const Tw *tw = a.tw1 + (size_t)m * N;
+    for (int st = a.logN - 1; st >= 0; --st) {
+        const int t = N >> (st + 1);
+        for (int b = tid; b < N / 2; b += kThreads) {
+            const int i = b / t, e = 2 * i * t + (b - i * t);
+            uint64_t U = s[e], V = s[e + t];
+            if (st == 0) {
+                // global stage 0 folds in N^-1
+                s[e] = shoup(U + V, md.ninv, md.ninv_sh, q);
+                s[e + t] = shoup(U + 2 * q - V, md.last, md.last_sh, q);
             } else {
-                int hs = S / 2;
-                int rr = b / hs;
-                int p = b - rr * hs;
-                i = p / t;
-                int j = p - i * t;
-                e = rr * S + 2 * i * t + j;
-                stride = t;
-                if (MODE == 0)
-                    w = tw1[(1 << st) + i];
-                else
-                    w = tw2[(size_t)(blockIdx.x * C + rr) * S + (1 << st) + i];
-            }
-            uint64_t U = s[e], V = s[e + stride];
-            if (last) {
-                uint64_t x = shoup(U + V, md.ninv, md.ninv_sh, q);
-                uint64_t y = shoup(U + 2 * q - V, md.last, md.last_sh, q);
-                s[e] = x;
-                s[e + stride] = y;
-            } else {
-                gs_bfly(U, V, w, q);
+                gs_bfly(U, V, tw[(1 << st) + i], q);
                 s[e] = U;
-                s[e + stride] = V;
+                s[e + t] = V;
             }
         }
         __syncthreads();
     }
-    if (MODE == 1) {
-        const int c0 = blockIdx.x * C;
-        for (int idx = tid; idx < total; idx += kThreads) {
-            int r = idx / C, cc = idx - r * C;
-            data[(long long)r * R + c0 + cc] = s[idx];
-        }
-    } else {
-        const long long off = (long long)blockIdx.x * total;
-        for (int idx = tid; idx < total; idx += kThreads) data[off + idx] = s[idx];
-    }
+    for (int idx = tid; idx < N; idx += kThreads) data[idx] = s[idx];
 }
 
 
@@ -1059,9 +930,9 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
             ProfScope ps(c, inverse ? PK_NTT_INV_FULL : PK_NTT_FWD_FULL, st, bytes);
             note_launch();
             if (inverse)
-                ntt_inv_kernel<0><<<grid, block, 0, st>>>(b);
+                ntt_inv_tile<<<grid, block, 0, st>>>(b);
             else
-                ntt_fwd_kernel<0><<<grid, block, 0, st>>>(b);
+                ntt_fwd_tile<<<grid, block, 0, st>>>(b);
         } else {
             switch (c.logN) {
             case 13: launch_phases<6, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
