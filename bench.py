@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--serve-parties16", type=int, default=16,
                     help="party-pool size of the logN=16 rings (64 for the full pool)")
     ap.add_argument("--serve-templates", type=int, default=96)
+    ap.add_argument("--serve-slots", type=int, default=8,
+                    help="requests the serving loop runs concurrently (slot streams)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -724,7 +726,7 @@ def run_serve(a, local, rank):
         outs = [ev.Ciphertext(P, k + 1, ref_level, False) for _ in range(2)]
         templates.append([("kklss", rlk, ops[0], ops[1], o) for o in outs])
     need = max(ev.job_scratch_bytes(t[0]) for t in templates)
-    slots = 8
+    slots = max(1, a.serve_slots)
     pool = int(min(max(need * 3, 8 << 30), 40 << 30))
     srv = ev.Server(device=local, scratch_bytes=pool, slots=slots, queue_cap=4096)
     # closed burst: capacity
