@@ -49,7 +49,7 @@ def test_mkf_ckks_logn13():
 
 
 def test_mkf_ckks_c1():
-    """BASELINE C1: CKKS logN=14, Q = 55b + 7x40b, P = 2x45b, k=2, scale 2^40."""
+    """Benchmark configuration C1: CKKS logN=14, Q = 55b + 7x40b, P = 2x45b, k=2, scale 2^40."""
     lit = params.get("ckks", "C1")
     case, got, lv, sc = _mkf_ckks(lit, 2, lit.max_level)
     prec = kg.precision_bits(H.mkf_ckks_decode(case, got, lv, sc), case.want)
@@ -57,7 +57,7 @@ def test_mkf_ckks_c1():
 
 
 def test_mkf_ckks_c3_k2_bitexact():
-    """BASELINE C3 parameters (logN=16, 24 Q limbs, 4 P limbs) at k=2, top level
+    """Benchmark configuration C3 parameters (logN=16, 24 Q limbs, 4 P limbs) at k=2, top level
     and level 8."""
     lit = params.get("ckks", "C3")
     case, got, lv, sc = _mkf_ckks(lit, 2, lit.max_level)
@@ -65,7 +65,7 @@ def test_mkf_ckks_c3_k2_bitexact():
 
 
 def test_mkf_bfv_c2_k4_bitexact():
-    """BASELINE C2: BFV logN=15, fifteen 58-bit Q, two 60-bit P, t=65537, k=4."""
+    """Benchmark configuration C2: BFV logN=15, fifteen 58-bit Q, two 60-bit P, t=65537, k=4."""
     lit = params.get("bfv", "C2")
     case = H.mkf_bfv_case(lit, 4, sparse=True)
     want = case.o.mkf_bfv_mulrelin(4, case.left, case.right, case.keys.fold, case.keys.relin, lit.t)
