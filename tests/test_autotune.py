@@ -24,6 +24,6 @@ def test_search_picks_the_fastest():
 
 
 def test_search_keeps_each_candidates_best_time():
-    times = iter([5.0, 1.0, 9.0, 2.0])  # round 1: a=5, b=1; round 2: a=9, b=2
+    times = iter([5.0, 1.0, 9.0, 2.0])  # sweep 1: a=5, b=1; sweep 2: a=9, b=2
     best, table = autotune.search([{"x": 0}, {"x": 1}], lambda c: next(times))
     assert best == {"x": 1} and table['{"x": 0}'] == 5.0 and table['{"x": 1}'] == 1.0
