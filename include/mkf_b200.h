@@ -5,8 +5,8 @@
  *     mkckks.Evaluator.MulRelinNew / Rescale, mkbfv.Evaluator.MulRelinNew,
  *     and the MKF aggregate-fold CKKSCase/BFVCase.Run / paper MulRelinNew
  * (ZhangChuanxin1/MKF, software/kklss/... and software/mkf/mkf_cpu/...).
- * A Go host binds it through cgo; every argument is a
- * plain pointer, size or scalar.  All entry points return an mkf_status;
+ * A Go host binds it through cgo; every argument is a plain pointer, size or
+ * scalar.  All entry points return an mkf_status;
  * mkf_last_error() gives the message of the last failure on a context.
  *
  * Data layout (the reference's fixture order, software/mkf/mkf_cpu/
@@ -369,7 +369,8 @@ mkf_status mkf_rescale(mkf_ctx *ctx, const mkf_ct *in, double min_scale, mkf_ct 
  * pay the device-wide synchronization of cudaFree).  Divides each of npolys
  * polynomials at `level` by its last modulus q_level (rounded), in the NTT
  * domain when is_ntt, else the coefficient domain: d_in [npolys][level+1][N]
- * and d_out [npolys][level][N] are caller-owned device buffers.  Temporaries
+ * and d_out [npolys][level][N] are caller-owned device buffers that must not
+ * overlap (the rescale does not run in place: MKF_ERR_INVALID_ARG).  Temporaries
  * live in one 8 MiB static device array shared by every call on a device:
  * at most 2^20 / (2N) polynomials per call; larger requests return
  * MKF_ERR_INVALID_ARG with a message.  The first call on a device looks up
@@ -412,6 +413,15 @@ uint64_t mkf_launch_count(int reset);
  * (moduli below 2^50).  Takes a few milliseconds; instrumentation for the
  * benchmark's compute roofline. */
 mkf_status mkf_probe_butterflies(int device, int kind, double *gbfly_per_s);
+
+/* Reduction schedule of the float64 NTT passes (instrumentation, no GPU
+ * needed): the bit mask the kernels are compiled with for a phase of 2^logs
+ * points whose input words are bounded by in16/16 q.  Forward (inverse = 0):
+ * bit p reduces after radix-8 pass p, bit 31 reduces the input; out16/16 q
+ * bounds the phase's output.  Inverse: bit st reduces the sum output of
+ * stage st; cols != 0 for the last phase (stage 0 folds in N^-1), else
+ * out16/16 q bounds the output. */
+unsigned mkf_ntt_f64_schedule(int inverse, int logs, int in16, int out16, int cols);
 
 #ifdef __cplusplus
 }

@@ -108,6 +108,7 @@ def lib():
         "mkf_version": (ctypes.c_char_p, []),
         "mkf_launch_count": (ctypes.c_uint64, [i]),
         "mkf_probe_butterflies": (i, [i, i, ctypes.POINTER(d)]),
+        "mkf_ntt_f64_schedule": (ctypes.c_uint, [i, i, i, i, i]),
         "mkf_ctx_create": (i, [ctypes.POINTER(ParamsDesc), ctypes.POINTER(vp)]),
         "mkf_ctx_destroy": (None, [vp]),
         "mkf_last_error": (i, [vp, ctypes.c_char_p, sz]),

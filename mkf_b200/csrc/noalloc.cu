@@ -26,7 +26,10 @@ std::mutex g_noalloc_mu;
 std::vector<uint64_t *> g_noalloc_ptr; // device address of the array, per device
 
 // Device address of g_noalloc_scratch for `device` (current).  The name is a
-// host-side stand-in in host code, so the address is queried once per device.
+// host-side stand-in in host code, so the address is queried once per device
+// and cached for the life of the process; a cudaDeviceReset while the library
+// is loaded would leave a stale address, so callers must not reset a device
+// they keep using through this entry point.
 cudaError_t noalloc_scratch(int device, uint64_t **out) {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     if ((int)g_noalloc_ptr.size() <= device) g_noalloc_ptr.resize(device + 1, nullptr);
@@ -100,6 +103,17 @@ extern "C" mkf_status mkf_rescale_noalloc(mkf_ctx *ctx, const uint64_t *d_in, ui
                                std::to_string(kNoAllocWords / (2 * N)) + " per call)");
         return MKF_ERR_INVALID_ARG;
     }
+    // the combine reads input limbs that later blocks or chunks still need
+    // while it writes the output: the two ranges must not overlap
+    {
+        const uintptr_t ib = (uintptr_t)d_in, ie = ib + (uintptr_t)npolys * (level + 1) * N * 8;
+        const uintptr_t ob = (uintptr_t)d_out, oe = ob + (uintptr_t)npolys * level * N * 8;
+        if (ib < oe && ob < ie) {
+            ctx_set_error(ctx, "mkf_rescale_noalloc: d_in and d_out overlap (the rescale cannot run "
+                               "in place)");
+            return MKF_ERR_INVALID_ARG;
+        }
+    }
     if (cudaSetDevice(c.device) != cudaSuccess) return MKF_ERR_CUDA;
     uint64_t *scratch = nullptr;
     cudaError_t e = noalloc_scratch(c.device, &scratch);
@@ -122,11 +136,18 @@ extern "C" mkf_status mkf_rescale_noalloc(mkf_ctx *ctx, const uint64_t *d_in, ui
     for (int i0 = 0; i0 < L; i0 += chunk) {
         const int n = std::min(chunk, L - i0);
         const dim3 grid((unsigned)((N + 255) / 256), n, npolys);
-        noalloc_spread_kernel<<<grid, block, 0, st>>>(last, L, i0, t, (long long)n * N, c.d_mods,
-                                                      (int)N);
+        {
+            ProfScope ps(c, PK_RESCALE, st, 16.0 * N * npolys * n);
+            noalloc_spread_kernel<<<grid, block, 0, st>>>(last, L, i0, t, (long long)n * N, c.d_mods,
+                                                          (int)N);
+        }
         if (is_ntt) ntt_forward(c, LimbSet{t, (long long)n * (long long)N, n, n, i0, 0}, npolys, st);
-        noalloc_combine_kernel<<<grid, block, 0, st>>>(d_in, in_ps, t, (long long)n * N, c.d_rescale,
-                                                       L, i0, d_out, out_ps, c.d_mods, (int)N, c.nQ);
+        {
+            ProfScope ps(c, PK_RESCALE, st, 24.0 * N * npolys * n);
+            noalloc_combine_kernel<<<grid, block, 0, st>>>(d_in, in_ps, t, (long long)n * N,
+                                                           c.d_rescale, L, i0, d_out, out_ps,
+                                                           c.d_mods, (int)N, c.nQ);
+        }
         note_launch(2);
     }
     e = cudaGetLastError();

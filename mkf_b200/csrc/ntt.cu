@@ -1225,6 +1225,13 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
     }
 }
 
+// Reduction schedules of the float64 passes as compiled (see fsched and
+// gsched above), for the instrumentation entry point below.
+unsigned ntt_f64_schedule(int inverse, int logs, int in16, int out16, int cols) {
+    if (logs < 1 || logs > 12 || in16 < 0 || out16 < 0) return 0u;
+    return inverse ? gsched::mask(logs, in16, cols != 0, out16) : fsched::mask(logs, in16, out16);
+}
+
 void ntt_forward(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st) {
     launch_split(c, ls, npolys, st, false);
 }
@@ -1233,3 +1240,7 @@ void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t s
 }
 
 } // namespace mkf
+
+extern "C" unsigned mkf_ntt_f64_schedule(int inverse, int logs, int in16, int out16, int cols) {
+    return mkf::ntt_f64_schedule(inverse, logs, in16, out16, cols);
+}
