@@ -39,13 +39,14 @@ METRIC = "mult+relin ops/s at logN=16,k=8: batched/served vs plain GPU; p50/p99 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mkf_b200", choices=["mkf_b200", "reference"])
     ap.add_argument("--config", default="C3")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--level", type=int, default=-1)
-    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--batch", type=int, default=48,
+                    help="products per step (48: at 20 steps the timed region lasts about 3 s)")
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--mix", type=int, default=512,
                     help="products in the mixed batch (k in {2,4,8,16}, logN in {14,15}, "
@@ -54,15 +55,23 @@ def parse():
     ap.add_argument("--tuning", default="",
                     help='launch choices as JSON, e.g. {"fuse_ip": 1, "ip_block": 256, '
                          '"modup_chunk": 24}, instead of autotuning (profiling runs)')
-    ap.add_argument("--serve-seconds", type=float, default=4.0,
-                    help="length of the open-loop Poisson trace; 0 skips serving")
+    ap.add_argument("--serve-seconds", type=float, default=6.0,
+                    help="length of each open-loop Poisson trace; 0 skips serving")
     ap.add_argument("--serve-rate", type=float, default=1000.0,
-                    help="offered load (req/s); capped at 0.8 x the measured capacity")
-    ap.add_argument("--serve-parties16", type=int, default=16,
-                    help="party-pool size of the logN=16 rings (64 for the full pool)")
+                    help="offered load (req/s) of the trace at load factor 1 when it is below "
+                         "the measured capacity; otherwise the capacity")
+    ap.add_argument("--serve-loads", default="0.8",
+                    help="load factors (x the offered load above) of the traces, e.g. "
+                         "0.5,0.8,1.0,1.2")
+    ap.add_argument("--serve-parties16", type=int, default=64,
+                    help="party-pool size of the logN=16 rings")
     ap.add_argument("--serve-templates", type=int, default=96)
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests the serving loop runs concurrently (slot streams)")
+    ap.add_argument("--served-seconds", type=float, default=3.0,
+                    help="open-loop trace of the headline product through the serving loop; "
+                         "0 skips it")
+    ap.add_argument("--served-slots", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -190,8 +199,25 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline (the oracle: test infrastructure, timed here as the baseline)
 # ---------------------------------------------------------------------------
-def _cpu_product_worker(args):
-    config, k, level, what, seed = args
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+_CPU_CASE = {}
+
+
+def _cpu_case(config, k, level, seed):
+    """Random keys and operands of one product (kept per worker process)."""
+    key_ = (config, k, level, seed)
+    if key_ in _CPU_CASE:
+        return _CPU_CASE[key_]
     sys.path.insert(0, ROOT)
     from mkf_b200 import params
     from oracle.oracle import Oracle
@@ -205,36 +231,55 @@ def _cpu_product_worker(args):
     L1 = level + 1
     key = np.stack([np.stack([np.concatenate([kg.uniform(g, lit.q, N), kg.uniform(g, lit.p, N)])
                               for _ in range(2)]) for _ in range(beta)])
-    if what == "switch":
-        x = kg.uniform(g, lit.q[:L1], N)
-        t0 = time.perf_counter()
-        o.mkf_switch_one(level, x, key, True, True)
-        return time.perf_counter() - t0
-    if what == "rescale":
-        x = kg.uniform(g, lit.q[:L1], N)
-        t0 = time.perf_counter()
-        o.rescale(level, x, True)
-        o.rescale(level, x, True)
-        return time.perf_counter() - t0
-    # full product
-    fold = np.stack([key] * k)
     left = np.stack([kg.uniform(g, lit.q[:L1], N) for _ in range(k + 1)])
     right = np.stack([kg.uniform(g, lit.q[:L1], N) for _ in range(k + 1)])
+    fold = np.ascontiguousarray(np.stack([key] * k))
+    _CPU_CASE.clear()
+    _CPU_CASE[key_] = (lit, o, key, fold, left, right)
+    return _CPU_CASE[key_]
+
+
+def _cpu_product_worker(args):
+    """One full MKF-CKKS mult+relin+rescale (fold of both operands with k
+    distinct fold-key slots, Karatsuba tensor, relinearization, rescale) by
+    the oracle on this process's core; 'switch' runs one switchOne only
+    (warm-up).  Returns the seconds it took."""
+    config, k, level, what, seed = args
+    lit, o, key, fold, left, right = _cpu_case(config, k, level, seed)
+    if what == "switch":
+        t0 = time.perf_counter()
+        o.mkf_switch_one(level, left[1], key, True, True)
+        return time.perf_counter() - t0
     t0 = time.perf_counter()
     o.mkf_ckks_mulrelin(k, level, left, right, fold, key, True, lit.scale, lit.scale ** 2)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(config, k, level):
-    """One full product on one core (about 15-25 s of CPU work)."""
-    t = _cpu_product_worker((config, k, level, "product", 7))
+def cpu_baseline(config, k, level, repeats=3):
+    """Full products on one core, the median of `repeats` (about 25 s)."""
+    times = [_cpu_product_worker((config, k, level, "product", 7)) for _ in range(repeats)]
+    t = statistics.median(times)
     return {"value": 1.0 / t, "unit": "mult+relin ops/s", "cores": 1, "kind": "port",
-            "sample": f"one full MKF-CKKS mult+relin+rescale ({config}, k={k}, level {level}) "
-                      f"by the C oracle on one core: {t:.2f} s"}
+            "cpu": cpu_model(), "repeats": repeats, "seconds": times,
+            "sample": f"one full MKF-CKKS mult+relin+rescale ({config}, k={k}, level {level}) by "
+                      f"the C oracle on one core, median of {repeats}: {t:.2f} s"}
+
+
+def _worker_count():
+    cores = os.cpu_count() or 1
+    try:
+        # each worker holds about 4 GB (keys, operands, the oracle's buffers)
+        mem_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES") / 1e9
+        return max(1, min(cores, int(mem_gb // 4)))
+    except (ValueError, OSError):
+        return cores
 
 
 def run_reference(a):
-    """--impl reference: the CPU restatement on every host core."""
+    """--impl reference: the reference algorithm's CPU restatement (the
+    oracle) on every host core.  A timed step runs one full product on each
+    worker process concurrently and lasts as long as the slowest of them;
+    warm-up steps run one switchOne per worker."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
@@ -242,34 +287,30 @@ def run_reference(a):
     from mkf_b200 import params
     lit = params.get("ckks", a.config)
     level = lit.max_level if a.level < 0 else a.level
-    cores = os.cpu_count() or 1
+    workers = _worker_count()
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        # per-product overhead beyond the 2k+1 switches, timed once
-        t_resc = pool.map(_cpu_product_worker, [(a.config, a.k, level, "rescale", 1)])[0]
+    with ctx.Pool(workers) as pool:
         for _ in range(max(1, a.warmup)):
-            pool.map(_cpu_product_worker, [(a.config, a.k, level, "switch", 10 + i) for i in range(cores)])
+            pool.map(_cpu_product_worker, [(a.config, a.k, level, "switch", 10 + i)
+                                           for i in range(workers)], chunksize=1)
         times = []
         for s in range(a.steps):
-            # the workers run concurrently; a step lasts as long as its slowest switch
-            r = pool.map(_cpu_product_worker, [(a.config, a.k, level, "switch", 100 + s * cores + i)
-                                               for i in range(cores)])
-            times.append(max(r))
-    t_step = sum(times) / len(times)
-    switches = 2 * a.k + 1
-    t_product = switches * t_step + t_resc  # wall time of `cores` products done in parallel
-    value = cores / t_product
-    sample = (f"each step: one MKF switchOne per worker on {cores} worker processes "
-              f"({a.config}, level {level}); a product = {switches} switches + a 2-poly rescale "
-              f"({t_resc:.2f} s, timed once)")
+            t0 = time.perf_counter()
+            pool.map(_cpu_product_worker, [(a.config, a.k, level, "product", 10 + i)
+                                           for i in range(workers)], chunksize=1)
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = workers * a.steps / total
+    sample = (f"each step: one full MKF-CKKS mult+relin+rescale ({a.config}, k={a.k}, level "
+              f"{level}) on each of {workers} worker processes at once, wall time of the step")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "mult+relin ops/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": total / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": f"MKF-CKKS mult+relin+rescale {a.config} logN=16 k={a.k} "
                                    f"level {level}", "parties": a.k, "level": level},
-            "cpu_baseline": {"value": value, "unit": "mult+relin ops/s", "cores": cores,
-                             "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "mult+relin ops/s", "cores": workers,
+                             "kind": "port", "cpu": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": "mult+relin ops/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "Go and Lattigo v2.3.0 are absent on this box; the reference algorithm is "
@@ -312,7 +353,10 @@ def run_gpu(a):
     ks = ev.MKFKeySet(P, [key() for _ in range(k)], key())
     E = ev.MKFEvaluator(P, ks)
     L1 = level + 1
-    nin = max(a.batch, 1)
+    streams = [torch.cuda.Stream() for _ in range(max(1, a.streams))]
+    # operand pairs cycled through by the products of a step; each stream
+    # writes its own output (its products run in order)
+    nin = max(8, len(streams))
     ins = []
     for _ in range(nin):
         l = ev.Ciphertext.from_array(P, random_limbs(g, lit.q[:L1], N, k + 1), True, scale=lit.scale)
@@ -327,12 +371,12 @@ def run_gpu(a):
     else:
         tuned = autotune.tune_mkf(P, k, level, operands=(E, ins[0][0], ins[0][1]))
     lout = E.output_level(ins[0][0], ins[0][1], True)
-    outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(nin)]
-    streams = [torch.cuda.Stream() for _ in range(max(1, a.streams))]
+    outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(len(streams))]
+    sidx = {s.cuda_stream: i for i, s in enumerate(streams)}
 
     def product(i, s):
         l, r = ins[i % nin]
-        E.MulRelin(l, r, outs[i % nin], rescale=True, materialize=True,
+        E.MulRelin(l, r, outs[sidx[s.cuda_stream]], rescale=True, materialize=True,
                    stream=ctypes_stream(s))
 
     barrier = reps.barrier
@@ -451,26 +495,29 @@ def run_gpu(a):
     if not a.no_e2e:
         words_in = (k + 1) * L1 * N
         words_out = (k + 1) * (lout + 1) * N
-        hin = [torch.empty(words_in, dtype=torch.int64, pin_memory=True) for _ in range(2 * a.batch)]
+        ns = len(streams)
+        # pinned host operands (two per stream, cycled) and one pinned output
+        # buffer and one set of device operands per stream
+        hin = [torch.empty(words_in, dtype=torch.int64, pin_memory=True) for _ in range(2 * ns)]
         for h in hin:
             h.numpy().view(np.uint64)[:] = g.integers(0, int(lit.q[-1]), size=words_in, dtype=np.uint64)
-        hout = [torch.empty(words_out, dtype=torch.int64, pin_memory=True) for _ in range(a.batch)]
+        hout = [torch.empty(words_out, dtype=torch.int64, pin_memory=True) for _ in range(ns)]
         e_ins = [(ev.Ciphertext(P, k + 1, level, True, scale=lit.scale),
-                  ev.Ciphertext(P, k + 1, level, True, scale=lit.scale)) for _ in range(a.batch)]
-        e_outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.batch)]
+                  ev.Ciphertext(P, k + 1, level, True, scale=lit.scale)) for _ in range(ns)]
+        e_outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(ns)]
 
         def e2e_step():
             for j in range(a.batch):
-                s = streams[j % len(streams)]
-                cs = ctypes_stream(s)
-                l, r = e_ins[j]
+                si = j % ns
+                cs = ctypes_stream(streams[si])
+                l, r = e_ins[si]
                 capi.check(P.handle, L.mkf_ct_upload_async(
-                    l.handle, ctypes.cast(hin[2 * j].data_ptr(), capi.u64p), words_in, cs))
+                    l.handle, ctypes.cast(hin[2 * si].data_ptr(), capi.u64p), words_in, cs))
                 capi.check(P.handle, L.mkf_ct_upload_async(
-                    r.handle, ctypes.cast(hin[2 * j + 1].data_ptr(), capi.u64p), words_in, cs))
-                E.MulRelin(l, r, e_outs[j], rescale=True, materialize=True, stream=cs)
+                    r.handle, ctypes.cast(hin[2 * si + 1].data_ptr(), capi.u64p), words_in, cs))
+                E.MulRelin(l, r, e_outs[si], rescale=True, materialize=True, stream=cs)
                 capi.check(P.handle, L.mkf_ct_download_async(
-                    e_outs[j].handle, ctypes.cast(hout[j].data_ptr(), capi.u64p), words_out, cs))
+                    e_outs[si].handle, ctypes.cast(hout[si].data_ptr(), capi.u64p), words_out, cs))
 
         fork()
         for _ in range(a.warmup):
@@ -500,11 +547,12 @@ def run_gpu(a):
                  ev.Ciphertext.from_array(P, random_limbs(g, lit.q[: l8 + 1], N, k + 1), True,
                                           scale=lit.scale)) for _ in range(nin)]
         lo8 = E.output_level(ins8[0][0], ins8[0][1], True)
-        outs8 = [ev.Ciphertext(P, k + 1, lo8, True) for _ in range(nin)]
+        outs8 = [ev.Ciphertext(P, k + 1, lo8, True) for _ in range(len(streams))]
 
         def product8(i, s):
             l, r = ins8[i % nin]
-            E.MulRelin(l, r, outs8[i % nin], rescale=True, materialize=True, stream=ctypes_stream(s))
+            E.MulRelin(l, r, outs8[sidx[s.cuda_stream]], rescale=True, materialize=True,
+                       stream=ctypes_stream(s))
 
         for i in range(a.warmup):
             product8(i, s0)
@@ -543,6 +591,7 @@ def run_gpu(a):
                 "latency_ms": {"p50": lat8[len(lat8) // 2],
                                "p99": lat8[min(len(lat8) - 1, int(0.99 * len(lat8)))]}}
 
+    served = run_served(a, local, P, E, ins, lout, k, plain_ops) if a.served_seconds > 0 else None
     mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
     serve = run_serve(a, local, rank) if a.serve_seconds > 0 else None
 
@@ -572,6 +621,7 @@ def run_gpu(a):
             "level8": lvl8,
             "autotune": {"best": tuned["best"],
                          "ms_per_product": tuned["ms"]},
+            "served": served,
             "batched_mix": mix,
             "serving": serve,
             "kernels": kinds,
@@ -665,6 +715,24 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
     batch_ms = timed(lambda: b.launch(cs), reps)
     kernels = int(L.mkf_launch_count(0)) // (reps + max(1, a.warmup))
     n = len(items)
+    # the same comparison per (ring, k) bucket: which products batching helps
+    buckets = {}
+    for name in ("S14", "S15"):
+        for kb in (2, 4, 8, 16):
+            sub = [it for it, sh in zip(items, shapes) if sh[0] == name and sh[1] == kb]
+            if not sub:
+                continue
+
+            def plain_sub(sub=sub):
+                for it in sub:
+                    it[1].MulRelin(it[2], it[3], it[4], rescale=True, materialize=True, stream=cs)
+
+            p_ms = timed(plain_sub, reps)
+            bb = ev.Batch(P0, sub, lanes=lanes, graph=True)
+            b_ms = timed(lambda: bb.launch(cs), reps)
+            bb.close()
+            buckets[f"{name}_k{kb}"] = {"products": len(sub), "plain_ms": p_ms, "batched_ms": b_ms,
+                                        "batched_over_plain": p_ms / b_ms}
     res = {"workload": f"{n} MK-CKKS mult+relin+rescale+materialize products, k uniform over "
                        "{2,4,8,16}, logN uniform over {14 (S14: 55b+7x40b, P 2x45b), "
                        "15 (S15: 60b+15x50b, P 4x60b)}, level uniform over [1,L]",
@@ -674,20 +742,92 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
                        "lanes": lanes, "graph": True, "kernels_per_launch": kernels},
            "batched_over_plain": plain_ms / batch_ms,
            "autotune_lanes_ms": tried,
+           "buckets": buckets,
            "mix": {f"k{k}": sum(1 for s in shapes if s[1] == k) for k in (2, 4, 8, 16)}}
     b.close()
     return res
 
 
+def poisson_trace(srv, templates, rate, seconds, g):
+    """Open-loop Poisson arrivals at `rate` req/s for `seconds` through the
+    serving loop; returns its statistics (latency: submit -> result complete
+    on the device)."""
+    srv.reset_stats()
+    n_req = max(1, int(rate * seconds))
+    gaps = g.exponential(1.0 / rate, size=n_req)
+    picks = g.integers(0, len(templates), size=n_req)
+    busy = 0
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i in range(n_req):
+        t_next += gaps[i]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        try:
+            srv.submit(templates[picks[i]][i % len(templates[picks[i]])])
+        except Exception as e:  # MKF_ERR_BUSY: the queue is full
+            if getattr(e, "status", None) != 8:
+                raise
+            busy += 1
+    srv.drain()
+    wall = time.perf_counter() - t_start
+    st = srv.stats()
+    return {"offered_req_s": rate, "seconds": seconds, "requests": n_req, "busy_rejected": busy,
+            "throughput_req_s": st["completed"] / wall if wall > 0 else None,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+            "inflight_peak": st["inflight_peak"],
+            "scratch_peak_gb": st["scratch_peak_bytes"] / 1e9}
+
+
+def run_served(a, local, P, E, ins, lout, k, plain_ops):
+    """The headline product (MKF-CKKS C3, k parties) through the serving loop
+    (mkf_server_*): a closed burst measures the served throughput with the
+    loop saturated, then an open-loop Poisson trace at 0.8 x that rate gives
+    p50/p99 latency.  Requests run on `--served-slots` slot streams with
+    scratch carved from one pool sized for that many products."""
+    from mkf_b200 import evaluator as ev
+    g = np.random.Generator(np.random.PCG64(4242))
+    slots = max(1, a.served_slots)
+    T = 2 * slots
+    outs = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(T)]
+    templates = [[("mkf", E, ins[i % len(ins)][0], ins[i % len(ins)][1], outs[i], True, True)]
+                 for i in range(T)]
+    need = ev.job_scratch_bytes(templates[0][0])
+    pool = need * slots + (64 << 20)
+    srv = ev.Server(device=local, scratch_bytes=pool, slots=slots, queue_cap=4096)
+    try:
+        for i in range(T):
+            srv.submit(templates[i][0])
+        srv.drain()
+        srv.reset_stats()
+        burst = 256
+        t0 = time.perf_counter()
+        for i in range(burst):
+            srv.submit(templates[i % T][0])
+        srv.drain()
+        capacity = burst / (time.perf_counter() - t0)
+        bst = srv.stats()
+        trace = poisson_trace(srv, templates, 0.8 * capacity, a.served_seconds, g)
+    finally:
+        srv.close()
+    return {"workload": "the headline product through the serving loop",
+            "value": capacity, "unit": "mult+relin ops/s", "slots": slots,
+            "scratch_pool_gb": pool / 1e9,
+            "burst": {"requests": burst, "p50_ms": bst["p50_ms"], "p99_ms": bst["p99_ms"]},
+            "served_over_plain": capacity / plain_ops,
+            "open_loop": trace}
+
+
 def run_serve(a, local, rank):
-    """Open-loop serving trace through the serving loop (mkf_server_*): KKLSS
+    """Open-loop serving traces through the serving loop (mkf_server_*): KKLSS
     mult+relin requests, scheme 50/50 CKKS/BFV, ring uniform over logN
     {14,15,16}, k uniform over {2..16} parties drawn from a per-ring key pool
     (64 parties at logN 14/15, `--serve-parties16` at 16), level uniform.
     Per-party relinearization keys are distinct HBM buffers.  Requests are
     drawn from `--serve-templates` prepared operand sets.  First a closed burst
-    measures capacity; then Poisson arrivals at min(rate, 0.8 x capacity)."""
-    import time
+    measures capacity; then Poisson arrivals at each load factor of
+    `--serve-loads` times min(rate, capacity)."""
     from mkf_b200 import capi, params
     from mkf_b200 import evaluator as ev
     g = np.random.Generator(np.random.PCG64(999 + rank))
@@ -743,43 +883,24 @@ def run_serve(a, local, rank):
     capacity = len(burst) / cap_s
     burst_stats = srv.stats()
     srv.reset_stats()
-    # open loop
-    rate = min(a.serve_rate, 0.8 * capacity)
-    n_req = max(1, int(rate * a.serve_seconds))
-    gaps = g.exponential(1.0 / rate, size=n_req)
-    picks = g.integers(0, len(templates), size=n_req)
-    tickets, busy = [], 0
-    t_start = time.perf_counter()
-    t_next = t_start
-    for i in range(n_req):
-        t_next += gaps[i]
-        dt = t_next - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        try:
-            tickets.append(srv.submit(templates[picks[i]][i % 2]))
-        except capi.MKFError as e:
-            if e.status != 8:
-                raise
-            busy += 1
-    srv.drain()
-    wall = time.perf_counter() - t_start
-    st = srv.stats()
+    # open loop, one trace per load factor
+    base = min(a.serve_rate, capacity)
+    traces = []
+    for f in [float(x) for x in a.serve_loads.split(",") if x]:
+        tr = poisson_trace(srv, templates, f * base, a.serve_seconds, g)
+        tr["load_factor"] = f
+        traces.append(tr)
     srv.close()
     return {"workload": "open-loop Poisson trace of KKLSS mult+relin requests: CKKS/BFV 50/50, "
                         "logN uniform over {14,15,16} (S14/S15/S16 sets), k uniform over {2..16} "
                         "from a per-ring party pool, level uniform (CKKS)",
-            "offered_req_s": rate, "requested_rate_req_s": a.serve_rate,
-            "seconds": a.serve_seconds, "requests": n_req, "busy_rejected": busy,
-            "throughput_req_s": st["completed"] / wall if wall > 0 else None,
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
-            "inflight_peak": st["inflight_peak"], "slots": slots,
-            "scratch_pool_gb": pool / 1e9, "scratch_peak_gb": st["scratch_peak_bytes"] / 1e9,
-            "key_pool_gb": key_bytes / 1e9,
+            "requested_rate_req_s": a.serve_rate, "slots": slots,
+            "scratch_pool_gb": pool / 1e9, "key_pool_gb": key_bytes / 1e9,
             "party_pool": {"logN14": 64, "logN15": 64, "logN16": a.serve_parties16},
             "capacity_req_s": capacity,
             "capacity_burst": {"requests": len(burst), "p50_ms": burst_stats["p50_ms"],
                                "p99_ms": burst_stats["p99_ms"]},
+            "traces": traces,
             "latency": "submit -> result complete on the device (host callback)"}
 
 

@@ -38,7 +38,8 @@ typedef enum mkf_status {
     MKF_ERR_LEVEL = 6,        /* level/scale precondition violated */
     MKF_ERR_TIMEOUT = 7,      /* a bounded device or host wait expired */
     MKF_ERR_BUSY = 8,         /* admission refused (server full) */
-    MKF_ERR_CANCELLED = 9     /* request cancelled before it ran */
+    MKF_ERR_CANCELLED = 9,    /* request cancelled before it ran */
+    MKF_ERR_CHECK = 10        /* debug build: a bounds or canary check failed */
 } mkf_status;
 
 enum { MKF_SCHEME_CKKS = 0, MKF_SCHEME_BFV = 1 };
@@ -261,6 +262,9 @@ typedef struct mkf_tuning {
     int fuse_ip;     /* 1: key-switch inner products fused into the digits' row pass */
     int ip_block;    /* threads per block of the stand-alone inner product: 128, 256, 512 */
     int modup_chunk; /* target limbs per thread of the party-summed ModUp: 8, 12, 24 */
+    int col_split;   /* blocks that share the limb walk of one column tile of the digit
+                      * column pass (limbs per block = ceil(limbs / col_split)): 1, 2, 4, 8 */
+    int ip_width;    /* coefficients per thread of the stand-alone inner product: 1, 2 */
 } mkf_tuning;
 mkf_status mkf_ctx_get_tuning(const mkf_ctx *ctx, mkf_tuning *out);
 mkf_status mkf_ctx_set_tuning(mkf_ctx *ctx, const mkf_tuning *t);
@@ -413,6 +417,18 @@ uint64_t mkf_launch_count(int reset);
  * (moduli below 2^50).  Takes a few milliseconds; instrumentation for the
  * benchmark's compute roofline. */
 mkf_status mkf_probe_butterflies(int device, int kind, double *gbfly_per_s);
+
+/* Debug build only (libmkf_b200_debug.so, compiled with MKF_DEBUG; no
+ * counterpart in the reference, which has no sanitizer either): every kernel
+ * index the checks cover (limb, coefficient, digit, party, twiddle and
+ * shared-memory positions) is bounds-checked, and every scratch allocation
+ * of an operation is followed by canary words written before and checked
+ * after it.  A failed check does not trap: it is counted and the access goes
+ * to an in-bounds word.  This call synchronizes `device`, fills report with
+ * {failures, first check tag, its value, its bound}, clears the records and
+ * returns MKF_OK when nothing failed, MKF_ERR_CHECK otherwise; the release
+ * build returns MKF_ERR_UNSUPPORTED. */
+mkf_status mkf_debug_status(int device, uint64_t *report);
 
 /* Reduction schedule of the float64 NTT passes (instrumentation, no GPU
  * needed): the bit mask the kernels are compiled with for a phase of 2^logs

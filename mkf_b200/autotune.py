@@ -2,12 +2,23 @@
 make a product fastest on the device at hand.
 
 The choices (mkf_tuning) never change the words computed, only the time:
-whether the key-switch inner products run fused into the digits' row pass
-or as their own memory-bound kernel, the inner-product block size, and the
-number of target limbs a thread of the party-summed ModUp handles.  The
-tuner times a product per candidate with CUDA events (after a warm-up),
-keeps the fastest, sets it on the context, and can keep the result in a JSON
-cache keyed by device and workload shape.
+
+* ``fuse_ip``: the key-switch inner products fused into the digits' row
+  pass, or run as their own memory-bound kernel;
+* ``ip_block`` and ``ip_width``: the key-switch tile of that kernel, threads
+  per block and coefficients per thread (2: 16-byte loads);
+* ``col_split``: limbs per block of the digit column pass (the blocks of a
+  column tile share its limb walk, ceil(limbs / col_split) limbs each);
+* ``modup_chunk``: target limbs per thread of the party-summed ModUp.
+
+The NTT's radix is fixed at 8 (three butterfly stages per pass on eight
+words held in registers), its phase split by the ring degree.
+
+The tuner times a product per candidate with CUDA events (after a warm-up)
+in a coordinate descent over the axes (each axis swept with the others held
+at their best so far, twice over), keeps the fastest, sets it on the
+context, and can keep the result in a JSON cache keyed by device and
+workload shape (ring degree, limbs, digits, parties).
 """
 from __future__ import annotations
 
@@ -21,7 +32,8 @@ import numpy as np
 
 from . import capi
 
-AXES = {"fuse_ip": (0, 1), "ip_block": (128, 256, 512), "modup_chunk": (8, 12, 24)}
+AXES = {"fuse_ip": (0, 1), "ip_block": (128, 256, 512), "modup_chunk": (8, 12, 24),
+        "col_split": (1, 2, 4, 8), "ip_width": (1, 2)}
 
 
 def candidates(axes: Dict[str, Iterable] = AXES) -> List[dict]:
@@ -38,7 +50,7 @@ def get_tuning(params) -> dict:
 def set_tuning(params, **kw):
     cur = get_tuning(params)
     cur.update(kw)
-    t = capi.Tuning(cur["fuse_ip"], cur["ip_block"], cur["modup_chunk"])
+    t = capi.Tuning(**{f: int(cur[f]) for f, _ in capi.Tuning._fields_})
     capi.check(params.handle, capi.lib().mkf_ctx_set_tuning(params.handle, ctypes.byref(t)))
 
 
@@ -57,11 +69,40 @@ def search(cands: List[dict], time_fn: Callable[[dict], float],
     return json.loads(best_key), table
 
 
+def descend(axes: Dict[str, Iterable], time_fn: Callable[[dict], float], start: dict,
+            rounds: int = 2) -> Tuple[dict, Dict[str, float]]:
+    """Coordinate descent: sweeps one axis at a time with the other axes at
+    their best value so far, `rounds` times over all axes.  Every point is
+    timed once per visit and keeps its best time; returns the best point and
+    the table of best times of every point visited."""
+    table: Dict[str, float] = {}
+    cur = dict(start)
+
+    def t(cnd):
+        k = json.dumps(cnd, sort_keys=True)
+        table[k] = min(table.get(k, float("inf")), float(time_fn(cnd)))
+        return table[k]
+
+    for _ in range(max(1, rounds)):
+        for ax, vals in axes.items():
+            best_v, best_t = cur[ax], None
+            for v in vals:
+                cnd = dict(cur, **{ax: v})
+                tv = t(cnd)
+                if best_t is None or tv < best_t:
+                    best_v, best_t = v, tv
+            cur[ax] = best_v
+    best_key = min(table, key=table.get)
+    return json.loads(best_key), table
+
+
 def _cache_key(params, k: int, level: int) -> str:
     import torch
     lit = params.literal
     name = torch.cuda.get_device_name(params.device) if torch.cuda.is_available() else "cpu"
-    return f"{name}|mkf-{params.scheme}|logN{lit.log_n}|Q{len(lit.q)}|P{len(lit.p)}|k{k}|L{level}"
+    beta = (level + len(lit.p)) // len(lit.p)
+    return (f"{name}|mkf-{params.scheme}|logN{lit.log_n}|Q{len(lit.q)}|P{len(lit.p)}|"
+            f"L{level + 1}|beta{beta}|k{k}")
 
 
 def tune_mkf(params, k: int, level: Optional[int] = None, reps: int = 4, keys=None, operands=None,
@@ -109,7 +150,10 @@ def tune_mkf(params, k: int, level: Optional[int] = None, reps: int = 4, keys=No
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
 
-    best, table = search(cands or candidates(), time_fn)
+    if cands is not None:
+        best, table = search(cands, time_fn)
+    else:
+        best, table = descend(AXES, time_fn, get_tuning(params))
     set_tuning(params, **best)
     res = {"best": best, "ms": table, "cached": False}
     if cache_path:

@@ -12,7 +12,9 @@ import re
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libmkf_b200.so")
+# MKF_B200_LIB=debug selects the debug build (bounds checks and canaries)
+LIB_PATH = os.path.join(HERE, "_lib", "libmkf_b200_debug.so"
+                        if os.environ.get("MKF_B200_LIB") == "debug" else "libmkf_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "mkf_b200.h")
 
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -23,7 +25,7 @@ OK = 0
 STATUS = {
     0: "MKF_OK", 1: "MKF_ERR_INVALID_ARG", 2: "MKF_ERR_CUDA", 3: "MKF_ERR_OOM",
     4: "MKF_ERR_UNSUPPORTED", 5: "MKF_ERR_MISSING_KEY", 6: "MKF_ERR_LEVEL",
-    7: "MKF_ERR_TIMEOUT", 8: "MKF_ERR_BUSY", 9: "MKF_ERR_CANCELLED",
+    7: "MKF_ERR_TIMEOUT", 8: "MKF_ERR_BUSY", 9: "MKF_ERR_CANCELLED", 10: "MKF_ERR_CHECK",
 }
 SCHEME = {"ckks": 0, "bfv": 1}
 KEY_SWITCHING, KEY_KKLSS_RLK, KEY_KKLSS_BFV_RLK, KEY_GADGET = 1, 2, 3, 4
@@ -69,7 +71,8 @@ class Job(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("fuse_ip", ctypes.c_int), ("ip_block", ctypes.c_int), ("modup_chunk", ctypes.c_int)]
+    _fields_ = [("fuse_ip", ctypes.c_int), ("ip_block", ctypes.c_int), ("modup_chunk", ctypes.c_int),
+                ("col_split", ctypes.c_int), ("ip_width", ctypes.c_int)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -109,6 +112,7 @@ def lib():
         "mkf_launch_count": (ctypes.c_uint64, [i]),
         "mkf_probe_butterflies": (i, [i, i, ctypes.POINTER(d)]),
         "mkf_ntt_f64_schedule": (ctypes.c_uint, [i, i, i, i, i]),
+        "mkf_debug_status": (i, [i, ctypes.POINTER(ctypes.c_uint64)]),
         "mkf_ctx_create": (i, [ctypes.POINTER(ParamsDesc), ctypes.POINTER(vp)]),
         "mkf_ctx_destroy": (None, [vp]),
         "mkf_last_error": (i, [vp, ctypes.c_char_p, sz]),

@@ -62,9 +62,31 @@ mkf_status call_scratch(Call &call, size_t *words) {
     return MKF_OK;
 }
 
+#ifdef MKF_DEBUG
+void dbg_guards_fill(uint64_t *base, const std::vector<size_t> &off, cudaStream_t st);
+void dbg_guards_check(uint64_t *base, const std::vector<size_t> &off, cudaStream_t st);
+#endif
+
+// Runs the call's launches on `st` over arena `a` (debug build: between the
+// canary fill and check of the guard regions its allocations leave).
+std::string run_body(Call &call, Arena &a, cudaStream_t st) {
+#ifdef MKF_DEBUG
+    Arena d;
+    d.dry = true;
+    d.used = a.used;
+    call.body(d, nullptr); // the same allocations, hence the same guard offsets
+    dbg_guards_fill(a.base, d.guards, st);
+    std::string e = call.body(a, st);
+    if (e.empty()) dbg_guards_check(a.base, d.guards, st);
+    return e;
+#else
+    return call.body(a, st);
+#endif
+}
+
 mkf_status run_call_arena(Call &call, cudaStream_t st, Arena &a) {
     cudaSetDevice(call.ctx->c.device);
-    std::string e = call.body(a, st);
+    std::string e = run_body(call, a, st);
     if (!e.empty()) return fail(call.ctx, status_of(e), e);
     mkf_status s = cuda_check(call.ctx, "kernel launch");
     if (s == MKF_OK && call.commit) call.commit();
@@ -87,7 +109,7 @@ mkf_status run_call(Call &call, cudaStream_t st) {
         if (!w->reserve(need)) return fail(ctx, MKF_ERR_OOM, "workspace allocation failed");
     }
     Arena a = w->arena();
-    std::string e = call.body(a, st);
+    std::string e = run_body(call, a, st);
     if (!e.empty()) return fail(ctx, status_of(e), e);
     s = cuda_check(ctx, "kernel launch");
     if (s == MKF_OK && call.commit) call.commit();
@@ -803,6 +825,8 @@ mkf_status mkf_ctx_get_tuning(const mkf_ctx *ctx, mkf_tuning *out) {
     out->fuse_ip = ctx->c.tune.fuse_ip;
     out->ip_block = ctx->c.tune.ip_block;
     out->modup_chunk = ctx->c.tune.modup_chunk;
+    out->col_split = ctx->c.tune.col_split;
+    out->ip_width = ctx->c.tune.ip_width;
     return MKF_OK;
 }
 
@@ -810,13 +834,17 @@ mkf_status mkf_ctx_set_tuning(mkf_ctx *ctx, const mkf_tuning *t) {
     if (!ctx || !t) return MKF_ERR_INVALID_ARG;
     if ((t->fuse_ip != 0 && t->fuse_ip != 1) ||
         (t->ip_block != 128 && t->ip_block != 256 && t->ip_block != 512) ||
-        (t->modup_chunk != 8 && t->modup_chunk != 12 && t->modup_chunk != 24))
+        (t->modup_chunk != 8 && t->modup_chunk != 12 && t->modup_chunk != 24) ||
+        (t->col_split != 1 && t->col_split != 2 && t->col_split != 4 && t->col_split != 8) ||
+        (t->ip_width != 1 && t->ip_width != 2))
         return fail(ctx, MKF_ERR_INVALID_ARG, "tuning values out of range");
     cudaSetDevice(ctx->c.device);
     cudaDeviceSynchronize(); // launches already queued keep their choices
     ctx->c.tune.fuse_ip = t->fuse_ip;
     ctx->c.tune.ip_block = t->ip_block;
     ctx->c.tune.modup_chunk = t->modup_chunk;
+    ctx->c.tune.col_split = t->col_split;
+    ctx->c.tune.ip_width = t->ip_width;
     return MKF_OK;
 }
 

@@ -66,6 +66,63 @@ struct LimbSet {
 
 #define MKF_DEV __device__ __forceinline__
 
+// ---------------------------------------------------------------------------
+// Debug build (-DMKF_DEBUG, libmkf_b200_debug.so): bounds checks on the
+// indices the kernels compute (limb, coefficient, digit, party, twiddle and
+// shared-memory positions).  A failed check never traps: it counts the
+// failure in this translation unit's device record, keeps the first failure
+// (tag, value, bound), and the access goes to index 0 of the same buffer, so
+// the context stays usable and the host reads the record afterwards
+// (mkf_debug_status).  In the release build the checks compile to nothing.
+// ---------------------------------------------------------------------------
+#ifdef MKF_DEBUG
+static __device__ unsigned long long g_mkf_dbg[4]; // failures, first tag, value, bound
+MKF_DEV void dbg_report(unsigned tag, unsigned long long v, unsigned long long bound) {
+    if (atomicAdd(&g_mkf_dbg[0], 1ull) == 0ull) {
+        g_mkf_dbg[1] = tag;
+        g_mkf_dbg[2] = v;
+        g_mkf_dbg[3] = bound;
+    }
+}
+template <typename I> MKF_DEV I dbg_idx(I v, unsigned long long bound, unsigned tag) {
+    if ((unsigned long long)(long long)v < bound) return v;
+    dbg_report(tag, (unsigned long long)(long long)v, bound);
+    return I(0);
+}
+// reads (and clears) this translation unit's record on the current device
+#define MKF_DBG_TU(name)                                                                           \
+    void dbg_collect_##name(unsigned long long *out) {                                             \
+        unsigned long long r[4] = {0, 0, 0, 0};                                                    \
+        cudaMemcpyFromSymbol(r, g_mkf_dbg, sizeof(r));                                             \
+        static const unsigned long long z[4] = {0, 0, 0, 0};                                       \
+        cudaMemcpyToSymbol(g_mkf_dbg, z, sizeof(z));                                               \
+        if (r[0] && !out[0]) {                                                                     \
+            out[1] = r[1];                                                                         \
+            out[2] = r[2];                                                                         \
+            out[3] = r[3];                                                                         \
+        }                                                                                          \
+        out[0] += r[0];                                                                            \
+    }
+#define MKF_DIDX(v, bound, tag) ::mkf::dbg_idx((v), (unsigned long long)(bound), (unsigned)(tag))
+#define MKF_DCHECK_LT(v, bound, tag)                                                               \
+    do {                                                                                           \
+        if (!((unsigned long long)(long long)(v) < (unsigned long long)(bound)))                   \
+            ::mkf::dbg_report((unsigned)(tag), (unsigned long long)(long long)(v),                 \
+                              (unsigned long long)(bound));                                        \
+    } while (0)
+#else
+#define MKF_DBG_TU(name)                                                                           \
+    void dbg_collect_##name(unsigned long long *) {}
+#define MKF_DIDX(v, bound, tag) (v)
+#define MKF_DCHECK_LT(v, bound, tag)                                                               \
+    do {                                                                                           \
+    } while (0)
+#endif
+// Check tags: the translation unit in the high byte, the site below it.
+enum : unsigned {
+    kDbgNtt = 0x01000000u, kDbgKernels = 0x02000000u, kDbgCanary = 0x0C000000u
+};
+
 MKF_DEV uint64_t mulhi64(uint64_t a, uint64_t b) { return __umul64hi(a, b); }
 
 // x*y*2^-64 mod q, canonical.

@@ -80,6 +80,8 @@ class Context {
         int fuse_ip = 0;       // inner products fused into the digits' row pass
         int ip_block = 256;    // threads per block of the inner-product kernel
         int modup_chunk = 12;  // target limbs per thread of the summed ModUp
+        int col_split = 4;     // blocks sharing a column tile's limb walk (digit column pass)
+        int ip_width = 1;      // coefficients per thread of the inner-product kernel
     } tune;
 
     int qidx(int i) const { return i; }

@@ -14,10 +14,19 @@ struct Arena {
     uint64_t *base = nullptr;
     size_t cap = 0, used = 0, peak = 0;
     bool dry = false;
+#ifdef MKF_DEBUG
+    // debug build: a guard region of canary words after every allocation
+    static constexpr size_t kGuard = 32;
+    std::vector<size_t> guards;
+#endif
     uint64_t *take(size_t words) {
         size_t w = (words + 31) & ~size_t(31); // 256-byte alignment
         size_t off = used;
         used += w;
+#ifdef MKF_DEBUG
+        guards.push_back(used);
+        used += kGuard;
+#endif
         if (used > peak) peak = used;
         if (dry) return reinterpret_cast<uint64_t *>(uintptr_t(256) + off * 8);
         return base + off;

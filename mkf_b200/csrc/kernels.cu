@@ -11,6 +11,9 @@
 
 namespace mkf {
 
+MKF_DBG_TU(kernels)
+
+
 constexpr int kBlock = 256;
 
 static inline dim3 grid_for(int N, int y = 1, int z = 1) {
@@ -242,10 +245,12 @@ bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride
 // ----------------------------------------------------------------------------
 // inner products
 // ----------------------------------------------------------------------------
-template <int NIN, int NOUT>
+// A thread owns W consecutive coefficients of one limb (W = 2: 16-byte
+// loads and stores) and every (input, output) accumulator of them.
+template <int NIN, int NOUT, int W>
 __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mods, int N,
                                                      int pmod0) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * W;
     if (x >= N) return;
     const int l = blockIdx.y, g = blockIdx.z;
     const bool isq = l < a.L1;
@@ -255,61 +260,101 @@ __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mod
     // B addressing: default B + g*b_gstride + t*b_tstride; per-group pointers
     // bptr[g] + t*b_tstride; per-term pointers bptr[t] + g*b_gstride
     const long long boff = (a.use_bptr && !a.bptr_per_term ? 0 : (long long)g * a.b_gstride) + blimb;
-    const uint64_t *Bg = a.use_bptr && !a.bptr_per_term ? a.bptr[g] : a.B;
-    Acc128 acc[NIN][NOUT];
+    const uint64_t *Bg = a.use_bptr && !a.bptr_per_term ? a.bptr[MKF_DIDX(g, 64, kDbgKernels | 1)] : a.B;
+    MKF_DCHECK_LT(l, a.L1 + a.nP, kDbgKernels | 2);
+    MKF_DCHECK_LT(a.nterms, a.bptr_per_term ? 65 : 1 << 20, kDbgKernels | 3);
+    Acc128 acc[NIN][NOUT][W];
 #pragma unroll
     for (int i = 0; i < NIN; ++i)
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) acc[i][o].zero();
+        for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+            for (int w = 0; w < W; ++w) acc[i][o][w].zero();
+    auto ldw = [](const uint64_t *p, uint64_t *v) {
+        if (W == 2) {
+            const ulonglong2 u = __ldg(reinterpret_cast<const ulonglong2 *>(p));
+            v[0] = u.x;
+            v[1] = u.y;
+        } else {
+            v[0] = __ldg(p);
+        }
+    };
     // terms in groups of TB: all loads of a group are issued before its MACs
-    constexpr int TB = 3;
-    auto load = [&](int t, uint64_t *bv, uint64_t *av) {
-        const uint64_t *bp = (a.bptr_per_term ? a.bptr[t] : Bg) + boff +
+    constexpr int TB = W == 1 ? 3 : 2;
+    auto load = [&](int t, uint64_t (*bv)[W], uint64_t (*av)[W]) {
+        const uint64_t *bp = (a.bptr_per_term ? a.bptr[MKF_DIDX(t, 64, kDbgKernels | 3)] : Bg) + boff +
                              (a.bptr_per_term ? 0 : (long long)t * a.b_tstride);
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) bv[o] = __ldg(bp + (long long)o * a.b_ostride);
+        for (int o = 0; o < NOUT; ++o) ldw(bp + (long long)o * a.b_ostride, bv[o]);
 #pragma unroll
         for (int i = 0; i < NIN; ++i)
-            av[i] = __ldg(a.A + aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride);
+            ldw(a.A + aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride, av[i]);
+    };
+    auto mac = [&](uint64_t (*bv)[W], uint64_t (*av)[W]) {
+#pragma unroll
+        for (int i = 0; i < NIN; ++i)
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+                for (int w = 0; w < W; ++w) acc[i][o][w].mac(av[i][w], bv[o][w], m.q);
     };
     int t = 0;
     for (; t + TB <= a.nterms; t += TB) {
-        uint64_t bv[TB][NOUT], av[TB][NIN];
+        uint64_t bv[TB][NOUT][W], av[TB][NIN][W];
 #pragma unroll
         for (int u = 0; u < TB; ++u) load(t + u, bv[u], av[u]);
 #pragma unroll
-        for (int u = 0; u < TB; ++u)
-#pragma unroll
-            for (int i = 0; i < NIN; ++i)
-#pragma unroll
-                for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av[u][i], bv[u][o], m.q);
+        for (int u = 0; u < TB; ++u) mac(bv[u], av[u]);
     }
     for (; t < a.nterms; ++t) {
-        uint64_t bv[NOUT], av[NIN];
+        uint64_t bv[NOUT][W], av[NIN][W];
         load(t, bv, av);
-#pragma unroll
-        for (int i = 0; i < NIN; ++i)
-#pragma unroll
-            for (int o = 0; o < NOUT; ++o) acc[i][o].mac(av[i], bv[o], m.q);
+        mac(bv, av);
     }
 #pragma unroll
     for (int i = 0; i < NIN; ++i)
 #pragma unroll
         for (int o = 0; o < NOUT; ++o) {
-            uint64_t r = mred128(acc[i][o].hi, acc[i][o].lo, m.q, m.qinv);
-            if (a.mform_out) r = mred(r, m.r2, m.q, m.qinv);
             uint64_t *op = a.out + (long long)g * a.out_gstride + (long long)i * a.out_istride +
                            (long long)o * a.out_ostride + (long long)l * N + x;
-            if (a.accumulate) r = add_mod(*op, r, m.q);
-            *op = r;
+            uint64_t r[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                r[w] = mred128(acc[i][o][w].hi, acc[i][o][w].lo, m.q, m.qinv);
+                if (a.mform_out) r[w] = mred(r[w], m.r2, m.q, m.qinv);
+            }
+            if (W == 2) {
+                ulonglong2 *o2 = reinterpret_cast<ulonglong2 *>(op);
+                if (a.accumulate) {
+                    const ulonglong2 prev = *o2;
+                    r[0] = add_mod(prev.x, r[0], m.q);
+                    r[W - 1] = add_mod(prev.y, r[W - 1], m.q);
+                }
+                *o2 = make_ulonglong2(r[0], r[W - 1]);
+            } else {
+                if (a.accumulate) r[0] = add_mod(*op, r[0], m.q);
+                *op = r[0];
+            }
         }
+}
+
+template <int W>
+static void launch_ip_w(const Context &c, const IpArgs &a, cudaStream_t st) {
+    const int blk = c.tune.ip_block;
+    dim3 grid((c.N / W + blk - 1) / blk, a.L1 + a.nP, a.groups);
+    const int pm = c.pidx(0);
+    if (a.nin == 1 && a.nout == 1)
+        ip_kernel<1, 1, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 1 && a.nout == 2)
+        ip_kernel<1, 2, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 2 && a.nout == 2)
+        ip_kernel<2, 2, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+    else if (a.nin == 2 && a.nout == 1)
+        ip_kernel<2, 1, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
 }
 
 void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
     if (a.groups <= 0 || a.nterms < 0) return;
-    const int blk = c.tune.ip_block;
-    dim3 grid((c.N + blk - 1) / blk, a.L1 + a.nP, a.groups);
-    const int pm = c.pidx(0);
     // algorithmic bytes: every digit word and key word read once, outputs written once
     const double lim = 8.0 * c.N * (a.L1 + a.nP);
     const bool bshared = !a.use_bptr && a.b_gstride == 0;
@@ -318,14 +363,10 @@ void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
                                 (double)a.groups * a.nin * a.nout * (a.accumulate ? 2 : 1));
     ProfScope ps(c, PK_IP, st, bytes);
     note_launch();
-    if (a.nin == 1 && a.nout == 1)
-        ip_kernel<1, 1><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
-    else if (a.nin == 1 && a.nout == 2)
-        ip_kernel<1, 2><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
-    else if (a.nin == 2 && a.nout == 2)
-        ip_kernel<2, 2><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
-    else if (a.nin == 2 && a.nout == 1)
-        ip_kernel<2, 1><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+    if (c.tune.ip_width == 2)
+        launch_ip_w<2>(c, a, st);
+    else
+        launch_ip_w<1>(c, a, st);
 }
 
 // ----------------------------------------------------------------------------
@@ -349,6 +390,7 @@ __global__ void __launch_bounds__(kBlock) modup_kernel(ModUpArgs a) {
     const uint64_t *src = a.src + (long long)blockIdx.y * a.src_pstride;
     uint64_t *out = a.out + (long long)blockIdx.y * a.out_pstride;
     uint64_t xs[MAXNS], y[MAXNS];
+    MKF_DCHECK_LT(a.tab.ns, MAXNS + 1, kDbgKernels | 4);
 #pragma unroll
     for (int i = 0; i < MAXNS; ++i)
         if (i < a.tab.ns) xs[i] = src[(long long)i * a.N + x];
@@ -406,6 +448,8 @@ __global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a, int c
     const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * ch;
     const int nj = min(ch, a.nt - j0);
     const int ns = a.tab.ns;
+    MKF_DCHECK_LT(ns, MAXNS + 1, kDbgKernels | 5);
+    MKF_DCHECK_LT(j0, a.nt, kDbgKernels | 6);
     // Y_i = sum over terms of y_i, kept below q_i; each wrap adds q_i, i.e.
     // Q to the reconstructed value, counted in wraps
     uint64_t Y[MAXNS];

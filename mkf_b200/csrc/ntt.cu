@@ -23,6 +23,8 @@
 
 namespace mkf {
 
+MKF_DBG_TU(ntt)
+
 constexpr int kTile = 4096;
 constexpr int kThreads = 256;
 
@@ -262,6 +264,7 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
         if (COLS) {
             const int r = idx / C, cc = idx % C;
             a = saddr<S>(cc, r);
+            MKF_DCHECK_LT(blockIdx.x * C + cc, R, kDbgNtt | 2);
             v = data[blockIdx.x * C + r * R + cc];
         } else {
             const int cc = idx / S, j = idx % S;
@@ -270,7 +273,7 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
         }
         if (CONV == 1) v = (uint64_t)__double_as_longlong(reduce_f(u64_to_f(v), qi, qd));
         if (CONV == 2) v = (uint64_t)__double_as_longlong(centered_f(v, (uint64_t)qd));
-        s[a] = v;
+        s[MKF_DIDX(a, kTile, kDbgNtt | 1)] = v;
     }
 }
 
@@ -317,7 +320,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = (REGIN && p == 0) ? vout[r] : s[saddr<S>(c, elem<LOGS>(p, t, r))];
+        for (int r = 0; r < 8; ++r) v[r] = (REGIN && p == 0) ? vout[r] : s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)];
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const int st = 3 * p + u;
@@ -326,7 +329,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
-                    const int i = twpos<LOGS>(p, u, t, r);
+                    const int i = MKF_DIDX(twpos<LOGS>(p, u, t, r), 1 << LOGS, kDbgNtt | 4);
                     const Tw w = TWS ? ldtw_s(tw + i) : ldtw(tw + i);
                     if (LAZY)
                         ct_bfly_lazy(v[r], v[r + stride], w, q);
@@ -340,7 +343,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
             for (int r = 0; r < 8; ++r) vout[r] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = v[r];
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = v[r];
             __syncwarp();
         }
     }
@@ -402,7 +405,7 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
 #pragma unroll
         for (int r = 0; r < 8; ++r)
             v[r] = (REGIN && p == 0) ? vout[r]
-                                     : __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+                                     : __longlong_as_double((long long)s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)]);
         if (p == 0 && (RED >> 31)) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
@@ -415,7 +418,7 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     if (r & stride) continue;
-                    const int i = twpos<LOGS>(p, u, t, r);
+                    const int i = MKF_DIDX(twpos<LOGS>(p, u, t, r), 1 << LOGS, kDbgNtt | 4);
                     const TwD w = TWS ? ldtwd_s(tw + i) : ldtwd(tw + i);
                     ct_bfly_f(v[r], v[r + stride], w, q);
                 }
@@ -430,7 +433,7 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
             for (int r = 0; r < 8; ++r) vout[r] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = (uint64_t)__double_as_longlong(v[r]);
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
             __syncwarp();
         }
     }
@@ -464,7 +467,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         const long long rowoff = (long long)(blockIdx.x * C + c) * S;
         uint64_t v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = data[rowoff + r * T + t];
+        for (int r = 0; r < 8; ++r) v[r] = data[MKF_DIDX(rowoff + r * T + t, N, kDbgNtt | 5)];
         // the last pass leaves the row in the warp's tile region; it is
         // stored from there in point order (lane t: points k*T + t)
         if (fp) {
@@ -565,8 +568,6 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
 constexpr int kColThreads = 256, kColWords = 2048;
 // dynamic shared memory: the exchange tile and one staged source limb
 constexpr size_t kColSmem = (size_t)kColWords * 8 * 2;
-// blocks per (poly, digit, column tile), each walking a share of the limbs
-constexpr int kColLimbSplit = 4;
 
 template <int LOGS>
 __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
         const uint64_t *xs = src.x + (long long)poly * src.x_pstride + (long long)start * N;
         for (int idx = tid; idx < NW; idx += kColThreads) {
             const int r = idx / C, cc = idx % C;
-            ys[cc * S + r] = xs[(long long)r * R + col0 + cc];
+            ys[MKF_DIDX(cc * S + r, NW, kDbgNtt | 6)] = xs[(long long)r * R + col0 + cc];
         }
     }
     __syncthreads();
@@ -654,6 +655,9 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             }
         } else {
             const int row = l < L1 ? l : src.nQ + (l - L1);
+            MKF_DCHECK_LT(l - L1 < 0 ? 0 : l - L1, limbs - L1 < 1 ? 1 : limbs - L1, kDbgNtt | 10);
+            MKF_DCHECK_LT(ns, src.alpha + 1, kDbgNtt | 8);
+            MKF_DCHECK_LT((long long)(col0 + c) * S + t + 7 * T, N, kDbgNtt | 7);
             const uint64_t *tvr = tb->vq + row * (ns + 1);
             const uint64_t *yl = src.y + (long long)pd * src.alpha * N + (long long)(col0 + c) * S + t;
             if (fp && tb->fp_src) {
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
                     vi[r] = (uint64_t)__double_as_longlong(
-                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + ((vpk[r >> 2] >> (8 * (r & 3))) & 0xffu)))),
+                        reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + MKF_DIDX((vpk[r >> 2] >> (8 * (r & 3))) & 0xffu, ns + 1, kDbgNtt | 9)))),
                                  md.qinvd, md.qd));
             } else {
                 // integer multSum, four words at a time
@@ -691,7 +695,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
                     for (int r = 0; r < 4; ++r) {
                         const uint64_t hh = __umul64hi(lo[r] * md.qinv, q);
                         const uint64_t x = canon3(
-                            hi[r] - hh + q + __ldg(tvr + ((vpk[(h + r) >> 2] >> (8 * ((h + r) & 3))) & 0xffu)), q);
+                            hi[r] - hh + q + __ldg(tvr + MKF_DIDX((vpk[(h + r) >> 2] >> (8 * ((h + r) & 3))) & 0xffu, ns + 1, kDbgNtt | 9)), q);
                         vi[h + r] = fp ? (uint64_t)__double_as_longlong(centered_f(x, q)) : x;
                     }
                 }
@@ -728,7 +732,7 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[saddr<S>(c, elem<LOGS>(p, t, r))];
+        for (int r = 0; r < 8; ++r) v[r] = s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)];
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -747,7 +751,7 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
                         U = x;
                         V = y;
                     } else {
-                        const int i = twpos<LOGS>(p, u, t, r);
+                        const int i = MKF_DIDX(twpos<LOGS>(p, u, t, r), 1 << LOGS, kDbgNtt | 4);
                         if (LAZY)
                             gs_bfly_lazy(U, V, ldtw(tw + i), q, bias);
                         else
@@ -757,7 +761,7 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
             }
         }
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = v[r];
+        for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = v[r];
         __syncwarp();
     }
 }
@@ -778,7 +782,7 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[saddr<S>(c, elem<LOGS>(p, t, r))]);
+        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)]);
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -794,15 +798,15 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
                         U = x;
                     } else {
                         if ((RED >> st) & 1)
-                            gs_bfly_f<true>(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
+                            gs_bfly_f<true>(U, V, ldtwd(tw + MKF_DIDX(twpos<LOGS>(p, u, t, r), 1 << LOGS, kDbgNtt | 4)), q, qi);
                         else
-                            gs_bfly_f<false>(U, V, ldtwd(tw + twpos<LOGS>(p, u, t, r)), q, qi);
+                            gs_bfly_f<false>(U, V, ldtwd(tw + MKF_DIDX(twpos<LOGS>(p, u, t, r), 1 << LOGS, kDbgNtt | 4)), q, qi);
                     }
                 }
             }
         }
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[saddr<S>(c, elem<LOGS>(p, t, r))] = (uint64_t)__double_as_longlong(v[r]);
+        for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
         __syncwarp();
     }
 }
@@ -828,7 +832,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
         const bool fp = md.q < kFp64Bound;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint64_t x = data[rowoff + k * T + t];
+            const uint64_t x = data[MKF_DIDX(rowoff + k * T + t, N, kDbgNtt | 5)];
             s[saddr<S>(c, k * T + t)] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
         }
         __syncwarp();
@@ -975,6 +979,10 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
     const long long rowoff = (long long)(blockIdx.x * C + c) * S;
     // accumulators of this row, point order (lane t: points k*T + t)
+    MKF_DCHECK_LT(c * S + t + 7 * T, kTile, kDbgNtt | 13);
+    MKF_DCHECK_LT(rowoff + t + 7 * T, N, kDbgNtt | 14);
+    MKF_DCHECK_LT(grp, 64, kDbgNtt | 12);
+    MKF_DCHECK_LT(l, a.ls.limbs, kDbgNtt | 11);
     uint64_t *acc0 = dsm + kTile + c * S + t;
     uint64_t *acc1 = acc0 + kTile;
 #pragma unroll
@@ -1125,7 +1133,7 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             sb.v = src.v + (long long)p0 * c.N;                                                    \
             sb.poly0 = first_poly;                                                                 \
             sb.own_out = b.ls.base;                                                                \
-            dim3 g1((1 << L2G) / (kColWords >> L1G), npp, kColLimbSplit);                          \
+            dim3 g1((1 << L2G) / (kColWords >> L1G), npp, c.tune.col_split);                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
             ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
@@ -1205,7 +1213,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         switch (c.logN) {
 #define MKF_DIGITS_CASE(LN, L1G, L2G)                                                              \
     case LN: {                                                                                     \
-        dim3 g1((1 << L2G) / (kColWords >> L1G), npp, kColLimbSplit), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
+        dim3 g1((1 << L2G) / (kColWords >> L1G), npp, c.tune.col_split), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \

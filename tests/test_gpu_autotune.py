@@ -29,6 +29,6 @@ def test_all_choices_compute_the_same_words(tmp_path):
         assert np.array_equal(got, ref), f"{cnd} differs"
     cache = str(tmp_path / "tune.json")
     res = autotune.tune_mkf(P, k, operands=(E, a, b), cache_path=cache)
-    assert res["best"] == autotune.get_tuning(P) and len(res["ms"]) == 18
+    assert res["best"] == autotune.get_tuning(P) and len(res["ms"]) >= 10
     again = autotune.tune_mkf(P, k, operands=(E, a, b), cache_path=cache)
     assert again["cached"] and again["best"] == res["best"]

@@ -21,6 +21,7 @@ import os
 import numpy as np
 import pytest
 
+from mkf_b200 import autotune
 from mkf_b200 import evaluator as ev
 from oracle import keygen as kg
 from tests import bench_cases as BC
@@ -57,18 +58,22 @@ def test_mkf_ckks_c3_k8_bitexact(name, oracle_results):
     lit = case.lit
     P = _params(lit, "ckks")
     E = ev.MKFEvaluator(P, ev.MKFKeySet(P, list(case.keys.fold), case.keys.relin))
-    out = E.MulRelinNew(ev.Ciphertext.from_array(P, case.left, True, scale=lit.scale),
-                        ev.Ciphertext.from_array(P, case.right, True, scale=lit.scale),
-                        materialize=True)
-    got = out.download()
+    left = ev.Ciphertext.from_array(P, case.left, True, scale=lit.scale)
+    right = ev.Ciphertext.from_array(P, case.right, True, scale=lit.scale)
     want, lv, sc = oracle_results[name].result()
-    assert out.Level() == lv == case.level - 1
-    assert abs(out.Scale - sc) <= 1e-9 * sc
-    assert got.shape[0] == case.k + 1
-    # the materialized form: C0, then Gamma once per party
-    assert_eq_mod(got[:2], want, lit.q[: lv + 1])
-    for i in range(2, case.k + 1):
-        assert np.array_equal(got[i], got[1])
+    # both inner-product forms the autotuner chooses between: stand-alone,
+    # and fused into the digits' row pass (the benchmark's choice)
+    for fuse in (0, 1):
+        autotune.set_tuning(P, fuse_ip=fuse)
+        out = E.MulRelinNew(left, right, materialize=True)
+        got = out.download()
+        assert out.Level() == lv == case.level - 1
+        assert abs(out.Scale - sc) <= 1e-9 * sc
+        assert got.shape[0] == case.k + 1
+        # the materialized form: C0, then Gamma once per party
+        assert_eq_mod(got[:2], want, lit.q[: lv + 1])
+        for i in range(2, case.k + 1):
+            assert np.array_equal(got[i], got[1])
     assert kg.precision_bits(H.mkf_ckks_decode(case, got, lv, sc), case.want) > 20
 
 

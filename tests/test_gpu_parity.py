@@ -23,7 +23,9 @@ _CTX = {}
 
 
 def gpu(lit, scheme):
-    key = (lit.name, scheme)
+    # keyed by the whole literal: small chains of one name can differ in
+    # their prime sizes
+    key = (lit, scheme)
     if key not in _CTX:
         _CTX[key] = ev.Parameters(lit, scheme)
     return _CTX[key]
