@@ -72,6 +72,9 @@ def parse():
                     help="open-loop trace of the headline product through the serving loop; "
                          "0 skips it")
     ap.add_argument("--served-slots", type=int, default=4)
+    ap.add_argument("--profile-products", type=int, default=0,
+                    help="profiling run: after --warmup products, run this many plain products of "
+                         "the headline workload (one stream) and exit; for ncu captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -381,6 +384,19 @@ def run_gpu(a):
 
     barrier = reps.barrier
     max_over_ranks = reps.max_over_ranks
+
+    if a.profile_products > 0:
+        for i in range(a.warmup):
+            product(i, streams[0])
+        torch.cuda.synchronize()
+        for i in range(a.profile_products):
+            product(i, streams[0])
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_products": a.profile_products, "tuning": tuned["best"],
+                              "config": a.config, "k": k, "level": level}), flush=True)
+        reps.close()
+        return
 
     # ---- plain: one product at a time on one stream -------------------------
     L = capi.lib()

@@ -224,6 +224,10 @@ MKF_DEV double reduce_f(double x, double qinv, double q) {
 MKF_DEV double u64_to_f(uint64_t v) {
     return __dadd_rn(__longlong_as_double((long long)(v | 0x4330000000000000ull)), -MKF_F_2P52);
 }
+// double holding an integer in [0, 2^52) -> uint64
+MKF_DEV uint64_t f_to_u64(double x) {
+    return (uint64_t)__double_as_longlong(__dadd_rn(x, MKF_F_2P52)) - 0x4330000000000000ull;
+}
 // canonical v in [0,q) -> the centered representative in (-q/2, q/2], as a double
 MKF_DEV double centered_f(uint64_t v, uint64_t q) {
     const long long x = (long long)(v > (q >> 1) ? v - q : v);

@@ -110,7 +110,8 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
 // (reconstructRNS, basis_extension.go:537-579), written column-major for the
 // digit column pass: coefficient r*2^n2 + cc goes to cc*2^n1 + r.  A block
 // reads a 32x32 tile of (r, cc) along cc and writes it along r through
-// shared memory.
+// shared memory.  A digit whose sources are all below 2^50 stores its y_i as
+// doubles (the same integers), the form its float64 multSum consumes.
 __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in, long long in_pstride,
                                                              const ModUpTab *tabs,
                                                              const DevModulus *mods, uint64_t *y,
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
     const int ns = (level > alpha * (d + 1) - 1 ? alpha - 2 : (level % alpha) - 1) + 2;
     if (ns < 2) return;
     const ModUpTab tab = tabs[d * (alpha + 1) + ns];
+    const bool yd = tab.fp_src != 0;
     const int ctiles = (1 << n2) / 32;
     const int r0 = (blockIdx.x / ctiles) * 32, c0 = (blockIdx.x % ctiles) * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
             for (int k = 0; k < 4; ++k) {
                 const uint64_t yi = mred(xs[i][k], inv, m.q, m.qinv);
                 vi[k] = __dadd_rn(vi[k], __ddiv_rn(__ull2double_rn(yi), m.qd));
-                tl[ty + 8 * k][tx] = yi;
+                tl[ty + 8 * k][tx] = yd ? (uint64_t)__double_as_longlong(u64_to_f(yi)) : yi;
             }
             __syncthreads();
 #pragma unroll

@@ -672,7 +672,9 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
                     const double cq = __ldg(tb->qmodd + (row * ns + i) * 2 + 1);
 #pragma unroll
                     for (int r = 0; r < 8; ++r)
-                        acc[r] = __dadd_rn(acc[r], mulmod_f(u64_to_f(__ldg(yl + (long long)i * N + r * T)), cw, cq, md.qd));
+                        acc[r] = __dadd_rn(acc[r], mulmod_f(__longlong_as_double(
+                                                                    (long long)__ldg(yl + (long long)i * N + r * T)),
+                                                                cw, cq, md.qd));
                 }
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
@@ -680,7 +682,13 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
                         reduce_f(__dadd_rn(acc[r], u64_to_f(__ldg(tvr + MKF_DIDX((vpk[r >> 2] >> (8 * (r & 3))) & 0xffu, ns + 1, kDbgNtt | 9)))),
                                  md.qinvd, md.qd));
             } else {
-                // integer multSum, four words at a time
+                // integer multSum, four words at a time.  The y_i of a digit
+                // whose sources are below 2^50 are stored as doubles: adding
+                // 2^52 puts the integer in the mantissa bits (and adding 0.0
+                // leaves the bits of a stored integer unchanged)
+                const bool yd = tb->fp_src != 0;
+                const double yoff = yd ? MKF_F_2P52 : 0.0;
+                const uint64_t ysub = yd ? 0x4330000000000000ull : 0ull;
 #pragma unroll
                 for (int h = 0; h < 8; h += 4) {
                     uint64_t lo[4], hi[4];
@@ -689,7 +697,12 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
                     for (int i = 0; i < ns; ++i) {
                         const uint64_t b = __ldg(tb->qmod + row * ns + i);
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) mac128(lo[r], hi[r], __ldg(yl + (long long)i * N + (h + r) * T), b);
+                        for (int r = 0; r < 4; ++r) {
+                            const uint64_t yv = (uint64_t)__double_as_longlong(__dadd_rn(
+                                                    __longlong_as_double((long long)__ldg(yl + (long long)i * N + (h + r) * T)),
+                                                    yoff)) - ysub;
+                            mac128(lo[r], hi[r], yv, b);
+                        }
                     }
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
@@ -967,8 +980,11 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
     extern __shared__ __align__(16) uint64_t dsm[];
     uint64_t *s = dsm;
+    // the inputs of one key group are adjacent blocks (blockIdx.x = row tile *
+    // nin + input), so the key rows one of them reads from HBM are still in
+    // L2 when the others read them: each key word crosses HBM about once
     const int l = blockIdx.y;
-    const int grp = blockIdx.z % g.groups, sidx = blockIdx.z / g.groups;
+    const int grp = blockIdx.z, sidx = blockIdx.x % g.nin, tile = blockIdx.x / g.nin;
     const int poly = sidx * g.groups + grp;
     const int m = a.ls.mod_of(l);
     const DevModulus md = a.mods[m];
@@ -977,7 +993,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const bool fp = q < kFp64Bound;
     const int N = 1 << a.logN;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
-    const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+    const long long rowoff = (long long)(tile * C + c) * S;
     // accumulators of this row, point order (lane t: points k*T + t)
     MKF_DCHECK_LT(c * S + t + 7 * T, kTile, kDbgNtt | 13);
     MKF_DCHECK_LT(rowoff + t + 7 * T, N, kDbgNtt | 14);
@@ -989,8 +1005,8 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     for (int k = 0; k < 8; ++k) acc0[k * T] = acc1[k * T] = 0;
     const uint64_t *kb = g.kptr[grp] ? g.kptr[grp] : g.B + (long long)grp * g.k_gstride;
     const long long krow = (long long)(l < g.L1 ? l : g.k_qlimbs + (l - g.L1)) * N + rowoff + t;
-    const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-    const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+    const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(tile * C + c) * S;
+    const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(tile * C + c) * S;
     if (fp) {
         // float64 limbs: the products with the keys (Montgomery forms) are
         // formed by mulvar_f on centered words and summed as doubles; the
@@ -1139,7 +1155,7 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
             if (p0) note_launch(1);                                                                \
         }                                                                                          \
-        dim3 g2((1 << L1G) / (kTile >> L2G), limbs, ip.groups * ip.nin);                           \
+        dim3 g2((1 << L1G) / (kTile >> L2G) * ip.nin, limbs, ip.groups);                           \
         ProfScope ps(c, PK_DIGITS_ROW_IP, st, bytes_row);                                          \
         smem_attr(ntt_digits_row_ip<L2G>, c.device, kRowIpSmem);                                   \
         note_launch(1);                                                                            \
