@@ -83,13 +83,15 @@ def parse():
 from mkf_b200.replicas import Replicas, dist_env  # noqa: E402
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, ncu, one launch)
-# of the fused decomposition + NTT column pass per source polynomial at
-# logN=16, L1=24, P=4 (C3 top level), and the pipe utilisation of the same
-# capture (profiles/digits_col_row_ip_c3_k2.md): 388.8 MB over 4 polynomials.
-DIGITS_COL_DRAM_PER_POLY = {(16, 24, 4): 388.813e6 / 4}
-DIGITS_COL_PIPES = {(16, 24, 4): {"fp64_cycles_active_pct": 34.3, "fmaheavy_cycles_active_pct": 33.3,
-                                  "issue_active_pct": 60.6}}
+def ncu_figures():
+    """Per-kernel figures of the committed ncu capture (profiles/ncu_kernels.json):
+    DRAM bytes per launch unit (dram__bytes_read.sum + dram__bytes_write.sum)
+    and pipe utilisation, with the command and commit that produced them."""
+    p = os.path.join(ROOT, "profiles", "ncu_kernels.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
 
 
 def digits_col_compute(L, device, lit, k, L1, nP, kinds):
@@ -489,20 +491,24 @@ def run_gpu(a):
     avg_ms = tk["ms"] / tk["launches"]
     bytes_per_launch = tk["bytes"] / tk["launches"]
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
-    shape = (lit.log_n, L1, nP)
-    traffic, pipes = None, None
-    if top[0] == "ntt_digits_col" and shape in DIGITS_COL_DRAM_PER_POLY:
-        # the fold launch (2k polynomials) and the relinearization launch (one)
-        # alternate, so a launch averages (2k+1)/2 source polynomials
-        traffic = DIGITS_COL_DRAM_PER_POLY[shape] * (2 * k + 1) / 2
-        pipes = DIGITS_COL_PIPES[shape]
+    traffic, pipes, traffic_src = None, None, None
+    nf = ncu_figures()
+    fig = (nf or {}).get("kernels", {}).get(top[0])
+    if fig and fig.get("shape") == [lit.log_n, L1, nP] and "dram_bytes_per_unit" in fig:
+        # DRAM traffic grows with the launch's units (source polynomials of the
+        # digit kernels); the fold launch (2k) and the relinearization launch
+        # (one) alternate, so a launch averages (2k+1)/2 of them
+        units = (2 * k + 1) / 2 if top[0].startswith("ntt_digits") else 1
+        traffic = fig["dram_bytes_per_unit"] * units
+        pipes = fig.get("pipes")
+        traffic_src = {"capture": nf.get("capture"), "scaled_by_units": units}
     roofline = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
                 "share": tk["ms"] / sum(v["ms"] for v in kinds.values()),
                 "limiter": "float64 and integer multiply pipes, not HBM",
-                "pipes_ncu": pipes,
+                "pipes_ncu": pipes, "traffic_source": traffic_src,
                 "compute": digits_col_compute(L, local, lit, k, L1, nP, kinds),
                 "timed_in": "profiled replay of the plain loop (one stream, no overlap)"}
 

@@ -3,17 +3,19 @@ constants (hardware/u55c/hls/include/par1_ckks_hls_constants.hpp and
 par1_bfv_hls_constants.hpp).  Those headers are the only in-tree values that
 Lattigo v2.3.0 itself produced for this path (exported by
 software/mkf/mkf_cpu/fpga_constants_test.go:114-240).  Run from the repository
-root with the reference checked out at REFERENCE (default /root/reference):
+root with the path of a checkout of the reference:
 
-    python tests/golden/make_golden.py [REFERENCE]
+    python tests/golden/make_golden.py REFERENCE
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-HDR = os.path.join(REF, "hardware", "u55c", "hls", "include")
+
+
+def header_dir(ref):
+    return os.path.join(ref, "hardware", "u55c", "hls", "include")
 
 
 def parse(path):
@@ -30,8 +32,11 @@ def parse(path):
 
 
 def main():
-    ckks = parse(os.path.join(HDR, "par1_ckks_hls_constants.hpp"))
-    bfv = parse(os.path.join(HDR, "par1_bfv_hls_constants.hpp"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE")
+    hdr = header_dir(sys.argv[1])
+    ckks = parse(os.path.join(hdr, "par1_ckks_hls_constants.hpp"))
+    bfv = parse(os.path.join(hdr, "par1_bfv_hls_constants.hpp"))
     doc = {
         "source": "hardware/u55c/hls/include/par1_{ckks,bfv}_hls_constants.hpp",
         "ckks": ckks,
