@@ -52,6 +52,8 @@ def parse():
                     help="products in the mixed batch (k in {2,4,8,16}, logN in {14,15}, "
                          "level uniform over [1,L]); 0 skips it")
     ap.add_argument("--lanes", default="4,8,16", help="lane counts the batch autotuner tries")
+    ap.add_argument("--plan-lanes", default="1,2",
+                    help="lane counts tried for the headline key-fused plan")
     ap.add_argument("--tuning", default="",
                     help='launch choices as JSON, e.g. {"fuse_ip": 1, "ip_block": 256, '
                          '"modup_chunk": 24}, instead of autotuning (profiling runs)')
@@ -334,11 +336,36 @@ def random_limbs(g, moduli, n, count=1):
     return out
 
 
-def run_gpu(a):
+def best_plan(ev, P, jobs, lanes_arg, cs, stream, reps=3):
+    """The key-fused batch plan (graph-captured) with the fastest lane count
+    of `lanes_arg`; returns (plan, lanes, {lanes: ms per launch})."""
+    tried, best = {}, None
+    for lanes in [int(x) for x in lanes_arg.split(",") if x]:
+        b = ev.Batch(P, jobs, lanes=lanes, graph=True, fuse_keys=True)
+        b.launch(cs)
+        e0, e1 = __import__("torch").cuda.Event(enable_timing=True), \
+            __import__("torch").cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            b.launch(cs)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tried[lanes] = ms
+        if best is None or ms < best[1]:
+            if best is not None:
+                best[0].close()
+            best = (b, ms, lanes)
+        else:
+            b.close()
+    return best[0], best[2], tried
+
+
+def run_c3(a, reps, ws, rank, local):
+    """The headline workload's sections (plain, streams, key-fused plan,
+    kernel breakdown, e2e, level 8, served).  Every device buffer of the
+    headline context is freed when this returns."""
     import torch
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    reps = Replicas("nccl", timeout_s=300)
     from mkf_b200 import capi, params
     from mkf_b200 import evaluator as ev
 
@@ -397,8 +424,7 @@ def run_gpu(a):
         if rank == 0:
             print(json.dumps({"profile_products": a.profile_products, "tuning": tuned["best"],
                               "config": a.config, "k": k, "level": level}), flush=True)
-        reps.close()
-        return
+        return None
 
     # ---- plain: one product at a time on one stream -------------------------
     L = capi.lib()
@@ -461,10 +487,6 @@ def run_gpu(a):
         batched_step(i)
     join()
     barrier()
-    L.mkf_launch_count(1)
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(streams[0])
@@ -475,10 +497,42 @@ def run_gpu(a):
     t1.record(streams[0])
     t1.synchronize()
     barrier()
+    streams_ms = max_over_ranks(t0.elapsed_time(t1))
+    streams_res = {"value": ws * a.steps * a.batch / (streams_ms / 1e3), "unit": "mult+relin ops/s",
+                   "ms_per_step": streams_ms / a.steps, "streams": len(streams),
+                   "form": "one call per product, products spread over the streams"}
+
+    # ---- batched (headline): the step's products as one key-fused plan ----------
+    # The products share the key bundle, so the plan runs them as fused calls
+    # (every stage one launch per group of products, every key read once per
+    # group), spread over lanes and replayed from one CUDA graph per step.
+    cs0 = ctypes_stream(s0)
+    pouts = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.batch)]
+    pjobs = [("mkf", E, ins[j % nin][0], ins[j % nin][1], pouts[j], True, True)
+             for j in range(a.batch)]
+    plan, plan_lanes, plan_tried = best_plan(ev, P, pjobs, a.plan_lanes, cs0, s0)
+    for _ in range(a.warmup):
+        plan.launch(cs0)
+    torch.cuda.synchronize()
+    barrier()
+    L.mkf_launch_count(1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t0.record(s0)
+    for step in range(a.steps):
+        plan.launch(cs0)
+    t1.record(s0)
+    t1.synchronize()
+    barrier()
     clk = clocks.stop()
     launches = int(L.mkf_launch_count(0))
     total_ms = max_over_ranks(t0.elapsed_time(t1))
     value = ws * a.steps * a.batch / (total_ms / 1e3)
+    plan_res = {"lanes": plan_lanes, "kernels_per_step": plan.kernels, "graph": True,
+                "fuse_keys": True, "lanes_ms_per_step": plan_tried}
+    plan.close()
+    del pouts, pjobs
 
     kinds = {}
     for i in range(nk):
@@ -607,47 +661,94 @@ def run_gpu(a):
         t1.synchronize()
         barrier()
         ms8 = max_over_ranks(t0.elapsed_time(t1))
+        pouts8 = [ev.Ciphertext(P, k + 1, lo8, True) for _ in range(a.batch)]
+        pjobs8 = [("mkf", E, ins8[j % nin][0], ins8[j % nin][1], pouts8[j], True, True)
+                  for j in range(a.batch)]
+        plan8, lanes8, _ = best_plan(ev, P, pjobs8, a.plan_lanes, cs0, s0)
+        for _ in range(a.warmup):
+            plan8.launch(cs0)
+        torch.cuda.synchronize()
+        barrier()
+        t0.record(s0)
+        for step in range(a.steps):
+            plan8.launch(cs0)
+        t1.record(s0)
+        t1.synchronize()
+        barrier()
+        pms8 = max_over_ranks(t0.elapsed_time(t1))
+        plan8.close()
+        del pouts8, pjobs8
         lat8.sort()
         lvl8 = {"level": l8, "plain": ws * plain_steps / (max_over_ranks(sum(lat8)) / 1e3),
-                "batched": ws * a.steps * a.batch / (ms8 / 1e3), "unit": "mult+relin ops/s",
+                "batched": ws * a.steps * a.batch / (pms8 / 1e3), "plan_lanes": lanes8,
+                "streams": ws * a.steps * a.batch / (ms8 / 1e3), "unit": "mult+relin ops/s",
                 "latency_ms": {"p50": lat8[len(lat8) // 2],
                                "p99": lat8[min(len(lat8) - 1, int(0.99 * len(lat8)))]}}
 
     served = run_served(a, local, P, E, ins, lout, k, plain_ops) if a.served_seconds > 0 else None
+    lat_sorted = sorted(lat)
+    return {
+        "value": value, "ms_per_step": total_ms / a.steps, "k": k, "level": level,
+        "streams": len(streams), "plain": {"value": plain_ops, "unit": "mult+relin ops/s"},
+        "batched_over_plain": value / plain_ops, "batched_form": plan_res, "streams_res": streams_res,
+        "latency_ms": {"p50": lat_sorted[len(lat) // 2],
+                       "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
+        "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "level8": lvl8,
+        "autotune": {"best": tuned["best"], "ms_per_product": tuned["ms"]},
+        "served": served, "kernels": kinds, "clocks": clk,
+    }
+
+
+def run_gpu(a):
+    import gc
+
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    reps = Replicas("nccl", timeout_s=300)
+    c3 = run_c3(a, reps, ws, rank, local)
+    if c3 is None:  # profiling run
+        reps.close()
+        return
+    gc.collect()
+    torch.cuda.synchronize()
+    barrier, max_over_ranks = reps.barrier, reps.max_over_ranks
     mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
+    gc.collect()
     serve = run_serve(a, local, rank) if a.serve_seconds > 0 else None
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a.config, k, level)
+        cpu = cpu_baseline(a.config, c3["k"], c3["level"])
 
     if rank == 0:
-        lat_sorted = sorted(lat)
+        k, level = c3["k"], c3["level"]
         line = {
-            "metric": METRIC, "value": value, "unit": "mult+relin ops/s", "n_gpus": ws,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+            "metric": METRIC, "value": c3["value"], "unit": "mult+relin ops/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": c3["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (uniform random key and ciphertext words)",
             "config": {"workload": f"MKF-CKKS mult+relin+rescale+materialize {a.config}: logN=16, "
                                    f"k={k}, Q=1x60b+23x50b, P=4x60b, level {level}",
                        "parties": k, "level": level, "batch_per_step": a.batch,
-                       "streams": len(streams), "l2": "inputs (keys 1.6 GB) larger than L2",
+                       "form": "key-fused batch plan replayed from a CUDA graph",
+                       "l2": "inputs (keys 1.6 GB) larger than L2",
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
-            "plain": {"value": plain_ops, "unit": "mult+relin ops/s"},
-            "batched_over_plain": value / plain_ops,
-            "latency_ms": {"p50": lat_sorted[len(lat) // 2],
-                           "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "e2e": e2e,
-            "gpu_launches": launches,
-            "roofline": roofline,
-            "level8": lvl8,
-            "autotune": {"best": tuned["best"],
-                         "ms_per_product": tuned["ms"]},
-            "served": served,
+            "plain": c3["plain"],
+            "batched_over_plain": c3["batched_over_plain"],
+            "batched_form": c3["batched_form"],
+            "streams": c3["streams_res"],
+            "latency_ms": c3["latency_ms"],
+            "e2e": c3["e2e"],
+            "gpu_launches": c3["gpu_launches"],
+            "roofline": c3["roofline"],
+            "level8": c3["level8"],
+            "autotune": c3["autotune"],
+            "served": c3["served"],
             "batched_mix": mix,
             "serving": serve,
-            "kernels": kinds,
-            "clocks": clk,
+            "kernels": c3["kernels"],
+            "clocks": c3["clocks"],
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -291,6 +291,13 @@ typedef struct mkf_job {
 } mkf_job;
 typedef struct mkf_batch mkf_batch;
 #define MKF_BATCH_GRAPH 1 /* capture the whole batch into one CUDA graph */
+/* Fuse MKF-CKKS jobs that share a key bundle, flags and operand level (both
+ * operands at it) into wider calls of up to 16 products each: every stage
+ * of the group is one launch, and every fold key and the relinearization key
+ * cross HBM once per group instead of once per product.  The group size is
+ * ceil(jobs of the bundle / lanes), capped at 16 and by the scratch the
+ * lanes may take (32 GiB in all); outputs stay bit-identical. */
+#define MKF_BATCH_FUSE_KEYS 2
 /* Validates every job (job.status; the first failure is returned and no
  * plan is made), spreads the jobs over `lanes` concurrent streams of their
  * context (longest job first onto the least-loaded lane), sizes each lane's

@@ -59,6 +59,7 @@ class ParamsDesc(ctypes.Structure):
 SLOT_MUL_ADD, SLOT_ADD_C0, SLOT_MUL = 0, 1, 2
 JOB_MKF, JOB_KKLSS = 1, 2
 BATCH_GRAPH = 1
+BATCH_FUSE_KEYS = 2
 
 
 class Job(ctypes.Structure):

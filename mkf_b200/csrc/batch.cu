@@ -10,8 +10,10 @@
 // plan is made; results are the single-call results bit for bit because
 // every job runs the same kernels on its own buffers.
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include <set>
+#include <tuple>
 
 #include "handles.h"
 
@@ -103,8 +105,53 @@ mkf_status mkf_batch_create(mkf_ctx *ctx, mkf_job *jobs, int n, int lanes, int f
         ctxs.insert(jc);
     }
     cudaSetDevice(b->device);
-    // longest job first onto the least-loaded lane
     lanes = std::max(1, std::min(lanes, std::max(n, 1)));
+    if (flags & MKF_BATCH_FUSE_KEYS) {
+        // MKF-CKKS jobs that share a key bundle, flags and operand level run
+        // as fused calls of G products each (mkf_ckks_mulrelin_multi)
+        std::map<std::tuple<const mkf_mkf_keyset *, int, int, int, long long>, std::vector<int>> groups;
+        std::vector<Call> units;
+        for (int i = 0; i < n; ++i) {
+            const mkf_job &j = jobs[i];
+            if (j.kind == MKF_JOB_MKF && j.a->ctx->c.scheme == MKF_SCHEME_CKKS &&
+                j.a->level == j.b->level)
+                groups[std::make_tuple(j.mkf_keys, j.flags, j.a->level, j.out->ncomp, j.out->cs())]
+                    .push_back(i);
+            else
+                units.push_back(b->calls[i]);
+        }
+        const double budget_words = 32.0 * (1ull << 30) / 8.0 / lanes;
+        for (auto &kv : groups) {
+            const std::vector<int> &idx = kv.second;
+            size_t w1 = 0;
+            mkf_status s = call_scratch(b->calls[idx[0]], &w1);
+            if (s != MKF_OK) return s;
+            const int cnt = (int)idx.size();
+            int G = std::min({kMaxOwnPtrs / 2, (cnt + lanes - 1) / lanes,
+                              std::max(1, (int)(budget_words / std::max<size_t>(w1, 1)))});
+            G = std::max(G, 1);
+            for (int g0 = 0; g0 < cnt; g0 += G) {
+                std::vector<const mkf_job *> js;
+                std::vector<Call *> singles;
+                for (int t = g0; t < std::min(cnt, g0 + G); ++t) {
+                    js.push_back(&jobs[idx[t]]);
+                    singles.push_back(&b->calls[idx[t]]);
+                }
+                if (js.size() == 1) {
+                    units.push_back(*singles[0]);
+                    continue;
+                }
+                Call fc;
+                s = prepare_mkf_fused(js[0]->a->ctx, js, singles, fc);
+                if (s != MKF_OK) return s;
+                units.push_back(fc);
+            }
+        }
+        b->calls.swap(units);
+        n = (int)b->calls.size();
+        lanes = std::max(1, std::min(lanes, std::max(n, 1)));
+    }
+    // longest job first onto the least-loaded lane
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(),

@@ -169,6 +169,51 @@ mkf_status prepare_mkf(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
     return MKF_OK;
 }
 
+mkf_status prepare_mkf_fused(mkf_ctx *ctx, const std::vector<const mkf_job *> &jobs,
+                             const std::vector<Call *> &singles, Call &call) {
+    if (jobs.empty() || jobs.size() != singles.size() || 2 * jobs.size() > (size_t)kMaxOwnPtrs)
+        return MKF_ERR_INVALID_ARG;
+    const mkf_job &j0 = *jobs[0];
+    const mkf_mkf_keyset *ks = j0.mkf_keys;
+    const int k = ks->k, level = j0.a->level, flags = j0.flags;
+    if (ctx->c.scheme != MKF_SCHEME_CKKS) return fail(ctx, MKF_ERR_INVALID_ARG, "fused products are CKKS");
+    std::vector<Operand> L, R;
+    std::vector<uint64_t *> outs;
+    for (const mkf_job *j : jobs) {
+        if (j->mkf_keys != ks || j->flags != flags || j->a->level != level || j->b->level != level ||
+            j->out->cs() != j0.out->cs() || j->out->ncomp != j0.out->ncomp)
+            return fail(ctx, MKF_ERR_INVALID_ARG, "fused products must share keys, flags and shapes");
+        L.push_back(Operand{j->a->d, j->a->cs(), j->a->ncomp, j->a->level});
+        R.push_back(Operand{j->b->d, j->b->cs(), j->b->ncomp, j->b->level});
+        outs.push_back(j->out->d);
+    }
+    int nb = 0;
+    double scale = j0.a->scale * j0.b->scale;
+    if (flags & MKF_FLAG_RESCALE) nb = rescale_count(ctx->c, level, ctx->c.scale, &scale);
+    const int n_out = (flags & MKF_FLAG_MATERIALIZE) ? k + 1 : 2;
+    KeyPtrs kp;
+    kp.k = k;
+    for (int i = 0; i < k; ++i) kp.p[i] = ks->fold[i];
+    const uint64_t *relin = ks->relin;
+    const long long ocs = j0.out->cs();
+    const int B = (int)jobs.size();
+    call.ctx = ctx;
+    call.body = [ctx, k, level, L, R, B, kp, relin, nb, n_out, outs, ocs](Arena &a, cudaStream_t st) {
+        return mkf_ckks_mulrelin_multi(ctx->c, a, st, k, level, L.data(), R.data(), B, kp, relin, nb,
+                                       n_out, outs.data(), ocs);
+    };
+    std::vector<std::function<void()>> commits;
+    call.cost = 0;
+    for (Call *c1 : singles) {
+        commits.push_back(c1->commit);
+        call.cost += c1->cost;
+    }
+    call.commit = [commits]() {
+        for (auto &f : commits) f();
+    };
+    return MKF_OK;
+}
+
 mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
                          const mkf_kklss_keyset *ks, mkf_ct *out, Call &call) {
     if (!ctx || !op0 || !op1 || !ks || !out) return MKF_ERR_INVALID_ARG;

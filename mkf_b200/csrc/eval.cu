@@ -151,7 +151,7 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
             own.p[s] = ops[s].data + ops[s].cs;
             own.pstride[s] = ops[s].cs;
         }
-        own.split = k;
+        own.per = k;
         ntt_inverse(c, lsq(f.coeff, poly, L1), nops * k, st);
     }
     bool fused = false;
@@ -197,12 +197,20 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     ip.out_istride = 2 * qp;
     ip.out_ostride = qp;
     ip.nterms = beta;
-    ip.nin = nops;
     ip.nout = 2;
     ip.groups = k;
     ip.L1 = L1;
     ip.nP = nP;
-    if (!fused) launch_ip(c, ip, st);
+    if (!fused) {
+        // the stand-alone kernel takes two inputs per launch
+        for (int s0 = 0; s0 < nops; s0 += 2) {
+            IpArgs ipp = ip;
+            ipp.nin = std::min(2, nops - s0);
+            ipp.A = f.dig + s0 * kk * beta * qp;
+            ipp.out = f.acc + s0 * 2 * qp;
+            launch_ip(c, ipp, st);
+        }
+    }
     // 3. ModDown summed over parties, then the fold
     if (!bfv)
         ntt_inverse(c, lsp_of_qp(c, f.acc, qp, L1), 2 * nops * k, st);
@@ -330,6 +338,118 @@ std::string kklss_galois(const Context &c, Arena &ar, cudaStream_t st, int k, in
     return "";
 }
 
+std::string mkf_ckks_mulrelin_multi(const Context &c, Arena &ar, cudaStream_t st, int k,
+                                   int level, const Operand *left, const Operand *right, int B,
+                                   const KeyPtrs &fold, const uint64_t *relin, int nb_rescale,
+                                   int n_out, uint64_t *const *out, long long out_cs) {
+    const int N = c.N, nQ = c.nQ, nP = c.nP, L1 = level + 1;
+    if (k < 1 || k > kMaxParties) return "party count out of range [1,64]";
+    if (level < 0 || level >= nQ) return "level out of range";
+    if (nP > 8) return "at most 8 special primes are supported";
+    if (B < 1 || 2 * B > kMaxOwnPtrs) return "products per fused call out of range [1,16]";
+    if (nb_rescale > level) return "cannot rescale below level 0";
+    if (n_out < 2) return "output needs at least two components";
+    for (int b = 0; b < B; ++b) {
+        if (left[b].ncomp < k + 1 || right[b].ncomp < k + 1)
+            return "operand has fewer than k+1 components";
+        if (left[b].level != level || right[b].level != level)
+            return "fused products need both operands at the product level";
+    }
+    const int beta = c.beta_of(level, 1);
+    const long long poly = (long long)L1 * N, qp = (long long)(L1 + nP) * N;
+    const int nops = 2 * B;
+    FoldScratch fs = take_fold_scratch(c, ar, false, k, level, nops);
+    uint64_t *F = ar.take(2LL * nops * poly);   // [nops][2][L1][N]
+    uint64_t *mu = ar.take(3LL * B * poly);     // [3][B][L1][N]: mu0, mu1, mu2 blocks
+    uint64_t *rcoef = ar.take((long long)B * poly);
+    uint64_t *rdig = ar.take((long long)B * beta * qp);
+    uint64_t *racc = ar.take(2LL * B * qp);     // [2][B][QP]
+    uint64_t *rtmp = ar.take(2LL * B * poly);
+    uint64_t *last = ar.take(2LL * B * N);
+    uint64_t *tr = ar.take(2LL * B * poly);
+    uint64_t *dscr = fs.dscr;
+    if (ar.dry) return "";
+
+    // 1-3. fold every operand of every product: F[s] = (C0_s + sum_i p0, sum_i p1)
+    Operand ops[kMaxOwnPtrs];
+    for (int b = 0; b < B; ++b) {
+        ops[2 * b] = left[b];
+        ops[2 * b + 1] = right[b];
+    }
+    fold_sides(c, st, false, k, level, ops, nops, fold, fs, F);
+    auto mu0 = [&](int b) { return mu + (long long)b * poly; };
+    auto mu1 = [&](int b) { return mu + (long long)(B + b) * poly; };
+    auto mu2 = [&](int b) { return mu + (long long)(2 * B + b) * poly; };
+    // 4. Karatsuba tensors in the NTT domain
+    for (int b = 0; b < B; ++b)
+        launch_karatsuba(c, F + 4LL * b * poly, F + (4LL * b + 1) * poly, F + (4LL * b + 2) * poly,
+                         F + (4LL * b + 3) * poly, mu0(b), mu1(b), mu2(b), L1, qmap(L1), st);
+    // 5. relinearize every mu2 with the aggregate key (read once for all)
+    d2d2(rcoef, poly, mu2(0), poly, poly, B, st);
+    ntt_inverse(c, lsq(rcoef, poly, L1), B, st);
+    bool rfused;
+    {
+        OwnNtt own;
+        own.p[0] = mu2(0);
+        own.pstride[0] = poly;
+        own.per = B;
+        DigitIpArgs g;
+        g.groups = 1;
+        g.nin = B;
+        g.B = relin;
+        g.k_tstride = 2LL * (nQ + nP) * N;
+        g.k_ostride = (long long)(nQ + nP) * N;
+        g.k_qlimbs = nQ;
+        g.out = racc;
+        g.out_istride = qp;
+        g.out_ostride = (long long)B * qp;
+        rfused = c.tune.fuse_ip && decompose_ntt_ip(c, rcoef, poly, level, beta, rdig, B, dscr, g, st, &own);
+        if (!rfused) decompose_ntt(c, rcoef, poly, 0, level, 1, beta, rdig, B, dscr, st, &own);
+    }
+    if (!rfused) {
+        IpArgs r;
+        r.A = rdig;
+        r.a_tstride = qp;
+        r.a_gstride = beta * qp;
+        r.B = relin;
+        r.b_tstride = 2LL * (nQ + nP) * N;
+        r.b_ostride = (long long)(nQ + nP) * N;
+        r.b_qlimbs = nQ;
+        r.out = racc;
+        r.out_gstride = qp;
+        r.out_ostride = (long long)B * qp;
+        r.nterms = beta;
+        r.nin = 1;
+        r.nout = 2;
+        r.groups = B;
+        r.L1 = L1;
+        r.nP = nP;
+        launch_ip(c, r, st);
+    }
+    // accumulator o of product b (index o*B + b) goes into mu_o of product b
+    moddown_prepare(c, st, racc, qp, 2 * B, L1, 1, rtmp);
+    launch_moddown_combine(c, pdown(c, racc, qp, rtmp, poly, mu, poly, 1), L1, qmap(L1), 2 * B, st);
+
+    // 6. rescale the mu0 and mu1 blocks (2B polynomials)
+    int lout = level;
+    for (int r = 0; r < nb_rescale; ++r) {
+        const int L = level - r;
+        d2d2(last, N, mu + (long long)L * N, poly, N, 2 * B, st);
+        ntt_inverse(c, lsq(last, N, 1, L), 2 * B, st);
+        launch_rescale_spread(c, last, N, L, tr, poly, 2 * B, st);
+        ntt_forward(c, lsq(tr, poly, L), 2 * B, st);
+        launch_rescale_combine(c, mu, poly, tr, poly, L, mu, poly, 2 * B, st);
+        lout = L - 1;
+    }
+    // 7. outputs: C0, then Gamma (materialized n_out - 1 times)
+    const long long wout = (long long)(lout + 1) * N;
+    for (int b = 0; b < B; ++b) {
+        d2d2(out[b], out_cs, mu0(b), poly, wout, 1, st);
+        launch_replicate(mu1(b), out[b] + out_cs, wout, n_out - 1, out_cs, st);
+    }
+    return "";
+}
+
 std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int scheme, int k,
                          int level, const Operand &left, const Operand &right,
                          const KeyPtrs &fold, const uint64_t *relin, int nb_rescale, int n_out,
@@ -344,6 +464,9 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
     if (left.ncomp < k + 1 || right.ncomp < k + 1) return "operand has fewer than k+1 components";
     if (left.level < level || right.level < level) return "operand level below the product level";
     if (n_out < 2) return "output needs at least two components";
+    if (!bfv && left.level == level && right.level == level)
+        return mkf_ckks_mulrelin_multi(c, ar, st, k, level, &left, &right, 1, fold, relin, nb_rescale,
+                                       n_out, &out, out_cs);
     const int beta = c.beta_of(level, 1);
     const long long poly = (long long)L1 * N, qp = (long long)NQP * N;
     const int nR = nQ + c.nQM;
@@ -438,7 +561,7 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         OwnNtt own;
         own.p[0] = mu2;
         own.pstride[0] = poly;
-        own.split = 1;
+        own.per = 1;
         DigitIpArgs g;
         g.groups = 1;
         g.nin = 1;

@@ -67,6 +67,16 @@ enum : int { kCKKS = 0, kBFV = 1 };
 // All functions return "" on success or an error message.  With ar.dry they
 // only size the scratch they need.
 
+// B MKF-CKKS products that share one key bundle (fold keys and relin key),
+// every operand at `level`, run as one product of wider launches: every fold
+// key and the relinearization key cross HBM once for all 2B operands, and
+// each stage is one launch for all products.  Bit-identical to B calls of
+// mkf_mulrelin.  B <= 16; out[b] receives product b.
+std::string mkf_ckks_mulrelin_multi(const Context &c, Arena &ar, cudaStream_t st, int k,
+                                   int level, const Operand *left, const Operand *right, int B,
+                                   const KeyPtrs &fold, const uint64_t *relin, int nb_rescale,
+                                   int n_out, uint64_t *const *out, long long out_cs);
+
 // MKF aggregate-fold mult+relin (software/mkf/mkf_cpu/ckks.go:102-166 and
 // bfv.go:212-252).  left/right: C0 + k components at `level` (CKKS: NTT
 // domain; BFV: coefficient domain, full level).  fold: per-party switching

@@ -84,6 +84,10 @@ mkf_status prepare_mkf(mkf_ctx *ctx, const mkf_ct *left, const mkf_ct *right,
                        const mkf_mkf_keyset *ks, int flags, mkf_ct *out, Call &call);
 mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
                          const mkf_kklss_keyset *ks, mkf_ct *out, Call &call);
+// One call for several validated MKF-CKKS jobs (singles: their own calls)
+// that share a key bundle, flags and operand level (mkf_ckks_mulrelin_multi).
+mkf_status prepare_mkf_fused(mkf_ctx *ctx, const std::vector<const mkf_job *> &jobs,
+                             const std::vector<Call *> &singles, Call &call);
 // Scratch words the call needs (dry run).
 mkf_status call_scratch(Call &call, size_t *words);
 // Issues the call on st, growing st's workspace first unless st is capturing.

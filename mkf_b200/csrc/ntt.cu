@@ -615,10 +615,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             // form, unless the fused row pass reads it from the input directly
             if (src.own_skip) continue;
             const int gp = src.poly0 + poly;
-            const uint64_t *xn = (gp < src.own.split
-                                      ? src.own.p[0] + (long long)gp * src.own.pstride[0]
-                                      : src.own.p[1] + (long long)(gp - src.own.split) * src.own.pstride[1]) +
-                                 (long long)l * N + col0;
+            const uint64_t *xn = src.own.poly(gp) + (long long)l * N + col0;
             uint64_t *od = src.own_out + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
             for (int idx = tid; idx < NW; idx += kColThreads) {
                 const long long o = (long long)(idx / C) * R + idx % C;
@@ -1020,10 +1017,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
                              l < start + digit_ns(g.level, g.alpha, d);
             double v[8];
             if (own) {
-                const uint64_t *xn = (poly < g.own.split
-                                          ? g.own.p[0] + (long long)poly * g.own.pstride[0]
-                                          : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
-                                     (long long)l * N + rowoff + t;
+                const uint64_t *xn = g.own.poly(poly) + (long long)l * N + rowoff + t;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) v[k] = centered_f(xn[k * T], q);
             } else {
@@ -1062,10 +1056,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
                              l < start + digit_ns(g.level, g.alpha, d);
             uint64_t v[8];
             if (own) {
-                const uint64_t *xn = (poly < g.own.split
-                                          ? g.own.p[0] + (long long)poly * g.own.pstride[0]
-                                          : g.own.p[1] + (long long)(poly - g.own.split) * g.own.pstride[1]) +
-                                     (long long)l * N + rowoff + t;
+                const uint64_t *xn = g.own.poly(poly) + (long long)l * N + rowoff + t;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) v[k] = xn[k * T];
             } else {

@@ -11,15 +11,21 @@ namespace mkf {
 // described by `ls`, in place.  Inputs canonical; outputs canonical.
 void ntt_forward(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
 
-// NTT-domain copies of the polynomials a decomposition reads (polynomials
-// below `split` from p[0], the others from p[1]).  A digit's own limbs are
-// then copied from them instead of being transformed again, as the
-// reference's DecomposeNTT does (Lattigo v2.3.0 rlwe.KeySwitcher.
-// DecomposeSingleNTT, called from software/mkf/mkf_cpu/common.go:82).
+// NTT-domain copies of the polynomials a decomposition reads: polynomial gp
+// is p[gp / per] + (gp % per) * pstride[gp / per] (one pointer per operand of
+// `per` polynomials).  A digit's own limbs are then copied from them instead
+// of being transformed again, as the reference's DecomposeNTT does (Lattigo
+// v2.3.0 rlwe.KeySwitcher.DecomposeSingleNTT, called from
+// software/mkf/mkf_cpu/common.go:82).
+constexpr int kMaxOwnPtrs = 32;
 struct OwnNtt {
-    const uint64_t *p[2] = {nullptr, nullptr};
-    long long pstride[2] = {0, 0};
-    int split = 0;
+    const uint64_t *p[kMaxOwnPtrs] = {};
+    long long pstride[kMaxOwnPtrs] = {};
+    int per = 1;
+    __host__ __device__ const uint64_t *poly(int gp) const {
+        const int g = gp / per;
+        return p[g] + (long long)(gp - g * per) * pstride[g];
+    }
 };
 
 // Source of the fused gadget-decomposition + NTT (logN >= 13).

@@ -370,9 +370,12 @@ class Batch:
     optionally captured into one CUDA graph.  Jobs are
     ("mkf", MKFEvaluator, left, right, out, rescale, materialize) or
     ("kklss", RelinearizationKeySet, op0, op1, out); outputs are shaped as for
-    the single calls (see MKFEvaluator.output_level / Evaluator.MulRelinNew)."""
+    the single calls (see MKFEvaluator.output_level / Evaluator.MulRelinNew).
+    fuse_keys: MKF-CKKS jobs that share a key bundle, flags and level run as
+    fused calls (each key read once per group; MKF_BATCH_FUSE_KEYS)."""
 
-    def __init__(self, params: Parameters, jobs, lanes: int = 8, graph: bool = True):
+    def __init__(self, params: Parameters, jobs, lanes: int = 8, graph: bool = True,
+                 fuse_keys: bool = False):
         self.params = params
         self._keep = list(jobs)  # handles must outlive the plan
         arr = (capi.Job * max(1, len(jobs)))()
@@ -390,8 +393,9 @@ class Batch:
             arr[i].a, arr[i].b, arr[i].out = left.handle, right.handle, out.handle
         self.jobs = arr
         h = ctypes.c_void_p()
-        st = capi.lib().mkf_batch_create(params.handle, arr, len(jobs), lanes,
-                                        capi.BATCH_GRAPH if graph else 0, ctypes.byref(h))
+        flags = (capi.BATCH_GRAPH if graph else 0) | (capi.BATCH_FUSE_KEYS if fuse_keys else 0)
+        st = capi.lib().mkf_batch_create(params.handle, arr, len(jobs), lanes, flags,
+                                        ctypes.byref(h))
         capi.check(params.handle, st)
         self.handle = h
 

@@ -128,3 +128,57 @@ def test_one_shot_batch(rings):
     capi.check(P.handle, capi.lib().mkf_mulrelin_batch(P.handle, arr, len(jobs), None))
     for i, j in enumerate(jobs):
         assert np.array_equal(j[4].download(), want[i]), f"job {i} differs"
+
+
+def _fused_jobs(ring, E, k, level, count, materialize):
+    jobs, singles = [], []
+    for _ in range(count):
+        left, right = ring.ct(k + 1, level, True), ring.ct(k + 1, level, True)
+        out = ev.Ciphertext(ring.P, k + 1 if materialize else 2, E.output_level(left, right, True),
+                            True)
+        jobs.append(("mkf", E, left, right, out, True, materialize))
+        singles.append(lambda E=E, l=left, r=right, m=materialize: E.MulRelinNew(l, r, True, m).download())
+    return jobs, singles
+
+
+@pytest.mark.parametrize("fuse_ip", [0, 1])
+@pytest.mark.parametrize("graph", [False, True])
+def test_key_fused_batch_matches_single_calls(rings, graph, fuse_ip):
+    """MKF_BATCH_FUSE_KEYS: products sharing a key bundle (two bundles, two
+    levels, compact and materialized outputs) run as fused calls of several
+    products, next to jobs that cannot fuse (KKLSS, another ring); every
+    output equals its single call, on both inner-product forms."""
+    from mkf_b200 import autotune
+    r14, r13 = rings
+    for r in rings:
+        autotune.set_tuning(r.P, fuse_ip=fuse_ip)
+    jobs, singles = [], []
+    for E, k, level, count, mat in [(r14.mkf[2], 2, 7, 7, True), (r14.mkf[3], 3, 5, 5, False),
+                                    (r14.mkf[2], 2, 4, 3, False), (r13.mkf[2], 2, 5, 4, True)]:
+        ring = r14 if E.params is r14.P else r13
+        j, s = _fused_jobs(ring, E, k, level, count, mat)
+        jobs += j
+        singles += s
+    extra, extra_singles = _make_jobs(r14, r13)
+    jobs += extra[-2:]  # the KKLSS jobs
+    singles += extra_singles[-2:]
+    want = [f() for f in singles]
+    b = ev.Batch(r14.P, jobs, lanes=2, graph=graph, fuse_keys=True)
+    assert b.statuses() == [0] * len(jobs)
+    import torch
+    for rep in range(2):
+        b.launch()
+        torch.cuda.synchronize()
+        for i, j in enumerate(jobs):
+            assert np.array_equal(j[4].download(), want[i]), \
+                f"job {i} differs (graph={graph}, fuse_ip={fuse_ip}, launch {rep})"
+    # fused calls issue far fewer kernels than one call per product
+    plain = ev.Batch(r14.P, jobs, lanes=2, graph=False)
+    plain.launch()
+    torch.cuda.synchronize()
+    if not graph:
+        assert b.kernels < plain.kernels
+    plain.close()
+    b.close()
+    for r in rings:
+        autotune.set_tuning(r.P, fuse_ip=0)
