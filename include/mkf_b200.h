@@ -336,6 +336,9 @@ typedef struct mkf_server_config {
     size_t scratch_bytes; /* request scratch pool */
     int slots;            /* requests in flight at most */
     int queue_cap;        /* queued requests at most (submit: MKF_ERR_BUSY) */
+    int fuse_max;         /* > 1: an admitted MKF-CKKS request takes up to fuse_max - 1
+                           * queued requests that share its key bundle, flags and
+                           * level into one fused call (MKF_BATCH_FUSE_KEYS); 0, 1: off */
 } mkf_server_config;
 typedef struct mkf_server_stats {
     uint64_t submitted, completed, failed, rejected, cancelled;

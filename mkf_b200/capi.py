@@ -78,7 +78,7 @@ class Tuning(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t),
-                ("slots", ctypes.c_int), ("queue_cap", ctypes.c_int)]
+                ("slots", ctypes.c_int), ("queue_cap", ctypes.c_int), ("fuse_max", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):

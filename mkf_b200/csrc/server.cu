@@ -72,7 +72,13 @@ struct ServerReq {
     mkf_server *srv = nullptr;
     uint64_t ticket = 0;
     Call call;
-    size_t words = 0, off = 0;
+    // key fusion: the job, whether it may fuse, and (for a leader) the fused
+    // call and the requests it carries besides itself
+    mkf_job job{};
+    bool fusable = false;
+    std::unique_ptr<Call> fused;
+    std::vector<ServerReq *> members;
+    size_t words = 0, off = 0, words1 = 0; // scratch (of the fused call), of the request alone
     int slot = -1, skipped = 0;
     Clock::time_point t_submit, t_done;
     mkf_status status = MKF_OK;
@@ -125,6 +131,47 @@ void complete(mkf_server *s, ServerReq *r) {
     s->last_done = r->t_done;
 }
 
+bool same_bundle(const ServerReq *a, const ServerReq *b) {
+    return a->job.mkf_keys == b->job.mkf_keys && a->job.flags == b->job.flags &&
+           a->job.a->level == b->job.a->level && a->job.out->ncomp == b->job.out->ncomp &&
+           a->job.out->cs() == b->job.out->cs();
+}
+
+// Gathers up to fuse_max - 1 queued requests behind `it` that share r's key
+// bundle into one fused call carried by r (lock held).  The group shrinks
+// until its scratch fits the free pool; a group of one is left as it was.
+void try_fuse(mkf_server *s, ServerReq *r, std::deque<ServerReq *>::iterator it) {
+    r->fused.reset();
+    r->members.clear();
+    r->words = r->words1;
+    std::vector<ServerReq *> cand;
+    for (auto jt = std::next(it); jt != s->queue.end() && (int)cand.size() < s->cfg.fuse_max - 1; ++jt)
+        if ((*jt)->fusable && same_bundle(r, *jt)) cand.push_back(*jt);
+    while (!cand.empty()) {
+        std::vector<const mkf_job *> jobs{&r->job};
+        std::vector<Call *> singles{&r->call};
+        for (ServerReq *m : cand) {
+            jobs.push_back(&m->job);
+            singles.push_back(&m->call);
+        }
+        std::unique_ptr<Call> fc(new Call());
+        size_t words = 0;
+        if (prepare_mkf_fused(r->job.a->ctx, jobs, singles, *fc) != MKF_OK ||
+            call_scratch(*fc, &words) != MKF_OK)
+            return;
+        words = (words + 31) & ~size_t(31);
+        size_t off = 0;
+        if (s->pool.alloc(words, &off)) {
+            s->pool.release(off, words); // taken again by the caller
+            r->fused = std::move(fc);
+            r->members = cand;
+            r->words = words;
+            return;
+        }
+        cand.resize(cand.size() / 2);
+    }
+}
+
 void scheduler(mkf_server *s) {
     cudaSetDevice(s->cfg.device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -134,7 +181,12 @@ void scheduler(mkf_server *s) {
         for (ServerReq *r : s->finished) {
             s->pool.release(r->off, r->words);
             s->slot_busy[r->slot] = 0;
-            s->inflight--;
+            s->inflight -= 1 + (int)r->members.size();
+            for (ServerReq *m : r->members) {
+                m->t_done = r->t_done;
+                m->status = r->status;
+                complete(s, m);
+            }
             complete(s, r);
         }
         if (!s->finished.empty()) s->cv_done.notify_all();
@@ -147,23 +199,25 @@ void scheduler(mkf_server *s) {
             if (fs == s->slot_busy.end()) break;
             ServerReq *r = *it;
             size_t off = 0;
+            if (r->fusable && s->cfg.fuse_max > 1) try_fuse(s, r, it);
             if (!s->pool.alloc(r->words, &off)) {
                 if (it == s->queue.begin() && ++r->skipped > kMaxBypass) break;
                 ++it;
                 continue;
             }
             it = s->queue.erase(it);
+            for (ServerReq *m : r->members) s->queue.erase(std::find(s->queue.begin(), s->queue.end(), m));
             r->off = off;
             r->slot = (int)(fs - s->slot_busy.begin());
             s->slot_busy[r->slot] = 1;
-            s->inflight++;
+            s->inflight += 1 + (int)r->members.size();
             s->inflight_peak = std::max(s->inflight_peak, s->inflight);
             cudaStream_t st = s->slots[r->slot];
             lk.unlock();
             Arena a;
             a.base = s->base + off;
             a.cap = r->words;
-            mkf_status ok = run_call_arena(r->call, st, a);
+            mkf_status ok = run_call_arena(r->fused ? *r->fused : r->call, st, a);
             cudaError_t e = cudaSuccess;
             if (ok == MKF_OK) e = cudaLaunchHostFunc(st, on_done, r);
             lk.lock();
@@ -176,7 +230,12 @@ void scheduler(mkf_server *s) {
                 r->t_done = Clock::now();
                 s->pool.release(r->off, r->words);
                 s->slot_busy[r->slot] = 0;
-                s->inflight--;
+                s->inflight -= 1 + (int)r->members.size();
+                for (ServerReq *m : r->members) {
+                    m->t_done = r->t_done;
+                    m->status = r->status;
+                    complete(s, m);
+                }
                 complete(s, r);
                 s->cv_done.notify_all();
             }
@@ -271,7 +330,10 @@ mkf_status mkf_server_submit(mkf_server *s, const mkf_job *job, uint64_t *ticket
         return st;
     }
     r->srv = s;
-    r->words = words;
+    r->words = r->words1 = words;
+    r->job = *job;
+    r->fusable = job->kind == MKF_JOB_MKF && jc->c.scheme == MKF_SCHEME_CKKS &&
+                 job->a->level == job->b->level;
     r->ticket = s->next_ticket++;
     r->t_submit = Clock::now();
     if (!s->any) {

@@ -449,8 +449,10 @@ class Server:
     wait for tickets, read p50/p99 latency and throughput."""
 
     def __init__(self, device: int = 0, scratch_bytes: int = 8 << 30, slots: int = 8,
-                 queue_cap: int = 4096):
-        cfg = capi.ServerConfig(device, scratch_bytes, slots, queue_cap)
+                 queue_cap: int = 4096, fuse_max: int = 0):
+        """fuse_max > 1: an admitted MKF-CKKS request takes up to fuse_max - 1
+        queued requests that share its key bundle into one fused call."""
+        cfg = capi.ServerConfig(device, scratch_bytes, slots, queue_cap, fuse_max)
         h = ctypes.c_void_p()
         st = capi.lib().mkf_server_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != capi.OK:

@@ -97,3 +97,34 @@ def test_server_cancels_queued_requests_on_close(rings):  # noqa: F811
     for _ in range(3):
         srv.submit(_fresh_out(jobs[0]))
     srv.close()  # must return: queued requests are cancelled, nothing in flight
+
+
+def test_server_fuses_requests_sharing_a_key_bundle(rings):  # noqa: F811
+    """fuse_max: queued MKF-CKKS requests of one key bundle are served as fused
+    calls; each result equals the product run alone, and the fused groups
+    keep requests of other bundles (and KKLSS requests) apart."""
+    from tests.test_gpu_batch import _fused_jobs
+    r14, r13 = rings
+    jobs, singles = [], []
+    for E, ring, k, level, count, mat in [(r14.mkf[2], r14, 2, 7, 6, True),
+                                          (r14.mkf[3], r14, 3, 5, 3, False),
+                                          (r13.mkf[2], r13, 2, 5, 4, True)]:
+        j, s = _fused_jobs(ring, E, k, level, count, mat)
+        jobs += j
+        singles += s
+    extra, extra_singles = _make_jobs(r14, r13)
+    jobs += extra[-2:]
+    singles += extra_singles[-2:]
+    want = [f() for f in singles]
+    srv = ev.Server(scratch_bytes=6 << 30, slots=2, queue_cap=256, fuse_max=4)
+    srv.pause(True)  # queue everything first, so that groups form
+    tickets = [srv.submit(j) for j in jobs]
+    srv.pause(False)
+    for i, t in enumerate(tickets):
+        st, _ = srv.wait(t, timeout_s=60)
+        assert st == capi.OK
+        assert np.array_equal(jobs[i][4].download(), want[i]), f"request {i} differs when fused"
+    s = srv.stats()
+    assert s["completed"] == len(jobs) and s["failed"] == 0
+    assert s["inflight_peak"] > 2  # more requests in flight than slots: groups ran
+    srv.close()
