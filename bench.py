@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--serve-parties16", type=int, default=64,
                     help="party-pool size of the logN=16 rings")
     ap.add_argument("--serve-templates", type=int, default=96)
+    ap.add_argument("--serve-hbm-gb", type=float, default=150.0,
+                    help="HBM budget of the serving trace: key pool plus request scratch")
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests the serving loop runs concurrently (slot streams)")
     ap.add_argument("--served-seconds", type=float, default=3.0,
@@ -80,6 +82,8 @@ def parse():
     ap.add_argument("--profile-products", type=int, default=0,
                     help="profiling run: after --warmup products, run this many plain products of "
                          "the headline workload (one stream) and exit; for ncu captures")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the KKLSS serving traces (no headline line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -709,6 +713,12 @@ def run_gpu(a):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     reps = Replicas("nccl", timeout_s=300)
+    if a.serve_only:
+        serve = run_serve(a, local, rank)
+        if rank == 0:
+            print(json.dumps({"metric": "KKLSS serving trace", "serving": serve}), flush=True)
+        reps.close()
+        return
     c3 = run_c3(a, reps, ws, rank, local)
     if c3 is None:  # profiling run
         reps.close()
@@ -1007,7 +1017,11 @@ def run_serve(a, local, rank):
         templates.append([("kklss", rlk, ops[0], ops[1], o) for o in outs])
     need = max(ev.job_scratch_bytes(t[0]) for t in templates)
     slots = max(1, a.serve_slots)
-    pool = int(min(max(need * 3, 8 << 30), 40 << 30))
+    # keys and request scratch share the HBM budget of the trace
+    pool = int(min(max(need * 3, 8 << 30), 40 << 30, a.serve_hbm_gb * 1e9 - key_bytes))
+    if pool < need:
+        raise SystemExit(f"serving: {key_bytes / 1e9:.1f} GB of keys leave no room for a "
+                         f"{need / 1e9:.1f} GB request under {a.serve_hbm_gb} GB")
     srv = ev.Server(device=local, scratch_bytes=pool, slots=slots, queue_cap=4096)
     # closed burst: capacity
     burst = [templates[i % len(templates)][i % 2] for i in range(2 * len(templates))]
@@ -1036,6 +1050,7 @@ def run_serve(a, local, rank):
                         "from a per-ring party pool, level uniform (CKKS)",
             "requested_rate_req_s": a.serve_rate, "slots": slots,
             "scratch_pool_gb": pool / 1e9, "key_pool_gb": key_bytes / 1e9,
+            "hbm_budget_gb": a.serve_hbm_gb,
             "party_pool": {"logN14": 64, "logN15": 64, "logN16": a.serve_parties16},
             "capacity_req_s": capacity,
             "capacity_burst": {"requests": len(burst), "p50_ms": burst_stats["p50_ms"],
