@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--profile-products", type=int, default=0,
                     help="profiling run: after --warmup products, run this many plain products of "
                          "the headline workload (one stream) and exit; for ncu captures")
+    ap.add_argument("--configs", type=int, default=1,
+                    help="1: also time C1 and C2 (plain GPU, oracle on one core)")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the KKLSS serving traces (no headline line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -728,6 +730,8 @@ def run_gpu(a):
     barrier, max_over_ranks = reps.barrier, reps.max_over_ranks
     mix = run_mix(a, local, rank, barrier, max_over_ranks) if a.mix > 0 else None
     gc.collect()
+    configs = run_configs(a, local) if a.configs and rank == 0 else None
+    gc.collect()
     serve = run_serve(a, local, rank) if a.serve_seconds > 0 else None
 
     cpu = None
@@ -759,6 +763,7 @@ def run_gpu(a):
             "autotune": c3["autotune"],
             "served": c3["served"],
             "batched_mix": mix,
+            "other_configs": configs,
             "serving": serve,
             "kernels": c3["kernels"],
             "clocks": c3["clocks"],
@@ -967,6 +972,80 @@ def run_served_one(a, local, P, E, ins, lout, k, plain_ops, slots, fuse_max):
             "burst": {"requests": burst, "p50_ms": bst["p50_ms"], "p99_ms": bst["p99_ms"]},
             "served_over_plain": capacity / plain_ops,
             "open_loop": trace}
+
+
+def run_configs(a, local):
+    """The other benchmark configurations, one product per call on one stream
+    (plain) and, for reference, the C oracle on one core: C1 (CKKS logN 14,
+    k 2, 55b + 7x40b, P 2x45b) and C2 (BFV logN 15, k 4, fifteen 58-bit Q and
+    QMul, P 2x60b, t 65537), in both constructions (MKF aggregate fold and
+    KKLSS per-party keys).  Synthetic uniform words."""
+    import torch
+    from mkf_b200 import capi, params
+    from mkf_b200 import evaluator as ev
+    from oracle.oracle import Oracle
+    res = {}
+    g = np.random.Generator(np.random.PCG64(31337))
+    st = torch.cuda.Stream()
+    cs = ctypes_stream(st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for cfg, scheme, k in (("C1", "ckks", 2), ("C2", "bfv", 4)):
+        lit = params.get(scheme, cfg)
+        P = ev.Parameters(lit, scheme, device=local)
+        nQ, nP, N = len(lit.q), len(lit.p), lit.n
+        qmin = min(min(lit.q), min(lit.p), min(lit.q_mul) if lit.q_mul else 1 << 62)
+        beta1 = (nQ + nP - 1) // nP
+        key = g.integers(0, qmin, size=(beta1, 2, nQ + nP, N), dtype=np.uint64)
+        level = lit.max_level
+        ops = g.integers(0, qmin, size=(2, k + 1, level + 1, N), dtype=np.uint64)
+        ckks = scheme == "ckks"
+        E = ev.MKFEvaluator(P, ev.MKFKeySet(P, [key] * k, key))
+        l = ev.Ciphertext.from_array(P, ops[0], ckks, scale=lit.scale if ckks else None)
+        r = ev.Ciphertext.from_array(P, ops[1], ckks, scale=lit.scale if ckks else None)
+        out = ev.Ciphertext(P, 2, E.output_level(l, r, ckks), ckks)
+        kind = capi.KEY_KKLSS_RLK if ckks else capi.KEY_KKLSS_BFV_RLK
+        rlk = ev.RelinearizationKeySet(P, g.integers(0, qmin, size=P.key_words(capi.KEY_GADGET),
+                                                      dtype=np.uint64))
+        img = g.integers(0, qmin, size=P.key_words(kind), dtype=np.uint64)
+        for pid in range(k):
+            rlk.AddRelinearizationKey(pid, img)
+        kl = ev.Ciphertext.from_array(P, ops[0], False, ids=list(range(k)),
+                                      scale=lit.scale if ckks else None)
+        kr = ev.Ciphertext.from_array(P, ops[1], False, ids=list(range(k)),
+                                      scale=lit.scale if ckks else None)
+        kout = ev.Evaluator(P).MulRelinNew(kl, kr, rlk)  # output shape; reused below
+        Lb = capi.lib()
+
+        def kklss():
+            capi.check(P.handle, Lb.mkf_kklss_mulrelin(P.handle, kl.handle, kr.handle, rlk.handle,
+                                                       kout.handle, cs))
+        row = {}
+        for name, fn in (("mkf", lambda: E.MulRelin(l, r, out, rescale=ckks, stream=cs)),
+                         ("kklss", kklss)):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            n = 20
+            e0.record(st)
+            for _ in range(n):
+                fn()
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / n
+            row[name] = {"plain_ops_s": 1e3 / ms, "ms": ms}
+        # the oracle, one core, one MKF product
+        o = Oracle.from_literal(lit)
+        fold = np.ascontiguousarray(np.stack([key] * k))
+        t0 = time.perf_counter()
+        if ckks:
+            o.mkf_ckks_mulrelin(k, level, ops[0], ops[1], fold, key, True, lit.scale, lit.scale ** 2)
+        else:
+            o.mkf_bfv_mulrelin(k, ops[0], ops[1], fold, key, lit.t)
+        row["mkf"]["cpu_oracle_s"] = time.perf_counter() - t0
+        row["workload"] = f"{scheme.upper()} {cfg}: logN {lit.log_n}, k {k}, level {level}"
+        res[cfg] = row
+        del E, l, r, out, kl, kr, kout, rlk, P
+    return res
 
 
 def run_serve(a, local, rank):
