@@ -211,6 +211,11 @@ MKF_DEV int swz(int j) {
     return j ^ ((((j >> 5) & 3) << 2) | (((j >> 4) & 1) << 1) | ((j >> 6) & 1));
 }
 template <int S> MKF_DEV int saddr(int c, int j) { return c * S + (swz(j) ^ (c & 15)); }
+// saddr is XOR-linear in the point index: swz only XORs bits 4-6 of j into
+// bits 0-3, and c*S has no bits below S, so for j = A | R with A and R on
+// disjoint bits, saddr<S>(c, A | R) = saddr<S>(c, A) ^ swz(R).  The passes
+// form a thread's base address once per pass and XOR in a per-register
+// constant (R = r << pass_pos, or k * T in point order).
 
 template <int LOGS> MKF_DEV constexpr int pass_pos(int p) {
     return LOGS - 3 * p - 3 > 0 ? LOGS - 3 * p - 3 : 0;
@@ -319,8 +324,9 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
     uint64_t v[8];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
+        const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = (REGIN && p == 0) ? vout[r] : s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)];
+        for (int r = 0; r < 8; ++r) v[r] = (REGIN && p == 0) ? vout[r] : s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)];
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const int st = 3 * p + u;
@@ -343,7 +349,7 @@ MKF_DEV void fwd_passes(uint64_t *s, const Tw *tw, uint64_t q, int c, int t,
             for (int r = 0; r < 8; ++r) vout[r] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = v[r];
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = v[r];
             __syncwarp();
         }
     }
@@ -402,10 +408,11 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
     double v[8];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
+        const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
         for (int r = 0; r < 8; ++r)
             v[r] = (REGIN && p == 0) ? vout[r]
-                                     : __longlong_as_double((long long)s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)]);
+                                     : __longlong_as_double((long long)s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)]);
         if (p == 0 && (RED >> 31)) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) v[r] = reduce_f(v[r], qi, q);
@@ -433,7 +440,7 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
             for (int r = 0; r < 8; ++r) vout[r] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
             __syncwarp();
         }
     }
@@ -453,6 +460,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     if (!COLS && a.own_alpha) {
         const int d = (blockIdx.y / limbs) % a.own_ndigits, start = d * a.own_alpha;
         if (l < a.ls.nq && l >= start && l < start + digit_ns(a.own_level, a.own_alpha, d)) return;
@@ -478,18 +486,18 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
             fwd_passes_f<LOGS, 32, 8, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[saddr<S>(c, k * T + t)]), md.qd);
+                data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[(sb0 ^ swz(k * T))]), md.qd);
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
                 fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
-                    data[rowoff + k * T + t] = reduce_any(s[saddr<S>(c, k * T + t)], q, md.one_sh);
+                    data[rowoff + k * T + t] = reduce_any(s[(sb0 ^ swz(k * T))], q, md.one_sh);
             } else {
                 fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[saddr<S>(c, k * T + t)], q);
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[(sb0 ^ swz(k * T))], q);
             }
         }
         return;
@@ -583,6 +591,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
     const int ns = digit_ns(src.level, src.alpha, d);
     const bool msum = ns >= 2 && src.tabs;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     const int col0 = blockIdx.x * C;
     // a one-limb digit's source limb is staged for the block's columns; the
     // y_i of a multSum digit are read from L2 for every limb
@@ -741,8 +750,9 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
     uint64_t v[8];
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
+        const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)];
+        for (int r = 0; r < 8; ++r) v[r] = s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)];
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -771,7 +781,7 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
             }
         }
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = v[r];
+        for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = v[r];
         __syncwarp();
     }
 }
@@ -791,8 +801,9 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
     double v[8];
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
+        const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)]);
+        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)]);
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -816,7 +827,7 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
             }
         }
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[MKF_DIDX(saddr<S>(c, elem<LOGS>(p, t, r)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
+        for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
         __syncwarp();
     }
 }
@@ -834,6 +845,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     if (!COLS) {
         // row phase: each row belongs to T lanes of one warp, loaded into and
         // stored from the warp's tile region in point order (lane t: points
@@ -843,13 +855,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const uint64_t x = data[MKF_DIDX(rowoff + k * T + t, N, kDbgNtt | 5)];
-            s[saddr<S>(c, k * T + t)] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
+            s[(sb0 ^ swz(k * T))] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
         }
         __syncwarp();
         if (fp) {
             inv_passes_f<LOGS, false>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md, c, t);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[saddr<S>(c, k * T + t)];
+            for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[(sb0 ^ swz(k * T))];
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
@@ -857,11 +869,11 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
                 // the first phase hands the second one values below 2q
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
-                    data[rowoff + k * T + t] = reduce_2q(s[saddr<S>(c, k * T + t)], md.q, md.one_sh);
+                    data[rowoff + k * T + t] = reduce_2q(s[(sb0 ^ swz(k * T))], md.q, md.one_sh);
             } else {
                 inv_passes<LOGS, false, false>(s, tw, md, c, t);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[saddr<S>(c, k * T + t)];
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[(sb0 ^ swz(k * T))];
             }
         }
         return;
@@ -990,6 +1002,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const bool fp = q < kFp64Bound;
     const int N = 1 << a.logN;
     const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     const long long rowoff = (long long)(tile * C + c) * S;
     // accumulators of this row, point order (lane t: points k*T + t)
     MKF_DCHECK_LT(c * S + t + 7 * T, kTile, kDbgNtt | 13);
@@ -1026,7 +1039,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
                 for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)src[r * T]);
                 fwd_passes_f<LOGS, 32, 64, false, false, true>(s, twd, md.qd, md.qinvd, c, t, v);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = __longlong_as_double((long long)s[saddr<S>(c, k * T + t)]);
+                for (int k = 0; k < 8; ++k) v[k] = __longlong_as_double((long long)s[(sb0 ^ swz(k * T))]);
             }
             const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
             const uint64_t *k1 = k0 + g.k_ostride;
@@ -1069,7 +1082,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
                 else
                     fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = s[saddr<S>(c, k * T + t)];
+                for (int k = 0; k < 8; ++k) v[k] = s[(sb0 ^ swz(k * T))];
             }
             const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
             const uint64_t *k1 = k0 + g.k_ostride;
