@@ -261,6 +261,10 @@ template <int LOGS, bool COLS, int CONV = 0>
 MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double qi = 0.0,
                        double qd = 0.0) {
     constexpr int S = 1 << LOGS, C = kTile / S;
+    // columns: element e of this thread is point e*S/8 + tid/C of column
+    // tid%C (kPhaseThreads is S/8 columns' worth), so its address is the
+    // thread's base XOR a constant
+    const int cbase = saddr<S>(tid % C, tid / C);
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const int idx = e * kPhaseThreads + tid;
@@ -268,7 +272,7 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
         int a;
         if (COLS) {
             const int r = idx / C, cc = idx % C;
-            a = saddr<S>(cc, r);
+            a = cbase ^ swz(e << (LOGS - 3));
             MKF_DCHECK_LT(blockIdx.x * C + cc, R, kDbgNtt | 2);
             v = data[blockIdx.x * C + r * R + cc];
         } else {
@@ -290,6 +294,7 @@ template <int LOGS, bool COLS>
 MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const DevModulus &md,
                         StoreRed red) {
     constexpr int S = 1 << LOGS, C = kTile / S;
+    const int cbase = saddr<S>(tid % C, tid / C); // as in tile_load
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const int idx = e * kPhaseThreads + tid;
@@ -297,7 +302,7 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
         long long o;
         if (COLS) {
             const int r = idx / C, cc = idx % C;
-            v = s[saddr<S>(cc, r)];
+            v = s[cbase ^ swz(e << (LOGS - 3))];
             o = blockIdx.x * C + r * R + cc;
         } else {
             const int cc = idx / S, j = idx % S;
