@@ -147,12 +147,13 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     OwnNtt own;
     if (!bfv) {
         for (int s = 0; s < nops; ++s) {
-            d2d2(f.coeff + s * kk * poly, poly, ops[s].data + ops[s].cs, ops[s].cs, poly, k, st);
             own.p[s] = ops[s].data + ops[s].cs;
             own.pstride[s] = ops[s].cs;
         }
         own.per = k;
-        ntt_inverse(c, lsq(f.coeff, poly, L1), nops * k, st);
+        // coefficient-domain copies of every party component, transformed
+        // straight out of the operands
+        ntt_inverse_from(c, own, lsq(f.coeff, poly, L1), nops * k, st);
     }
     bool fused = false;
     if (c.tune.fuse_ip && (!bfv || nops == 1)) {
@@ -385,14 +386,13 @@ std::string mkf_ckks_mulrelin_multi(const Context &c, Arena &ar, cudaStream_t st
         launch_karatsuba(c, F + 4LL * b * poly, F + (4LL * b + 1) * poly, F + (4LL * b + 2) * poly,
                          F + (4LL * b + 3) * poly, mu0(b), mu1(b), mu2(b), L1, qmap(L1), st);
     // 5. relinearize every mu2 with the aggregate key (read once for all)
-    d2d2(rcoef, poly, mu2(0), poly, poly, B, st);
-    ntt_inverse(c, lsq(rcoef, poly, L1), B, st);
     bool rfused;
     {
         OwnNtt own;
         own.p[0] = mu2(0);
         own.pstride[0] = poly;
         own.per = B;
+        ntt_inverse_from(c, own, lsq(rcoef, poly, L1), B, st);
         DigitIpArgs g;
         g.groups = 1;
         g.nin = B;
@@ -434,8 +434,11 @@ std::string mkf_ckks_mulrelin_multi(const Context &c, Arena &ar, cudaStream_t st
     int lout = level;
     for (int r = 0; r < nb_rescale; ++r) {
         const int L = level - r;
-        d2d2(last, N, mu + (long long)L * N, poly, N, 2 * B, st);
-        ntt_inverse(c, lsq(last, N, 1, L), 2 * B, st);
+        OwnNtt lastL; // limb L of the mu0 and mu1 blocks
+        lastL.p[0] = mu + (long long)L * N;
+        lastL.pstride[0] = poly;
+        lastL.per = 2 * B;
+        ntt_inverse_from(c, lastL, lsq(last, N, 1, L), 2 * B, st);
         launch_rescale_spread(c, last, N, L, tr, poly, 2 * B, st);
         ntt_forward(c, lsq(tr, poly, L), 2 * B, st);
         launch_rescale_combine(c, mu, poly, tr, poly, L, mu, poly, 2 * B, st);

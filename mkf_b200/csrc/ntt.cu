@@ -39,6 +39,10 @@ struct NttArgs {
     // row pass of gadget digits [poly][digit][limb]: skip each digit's own
     // limbs (already final, copied by the column pass); 0 = transform all
     int own_alpha = 0, own_ndigits = 0, own_level = 0;
+    // inverse transform out of place: the first pass reads polynomial
+    // src_poly0 + i from src (see OwnNtt) and writes ls; -1: in place
+    OwnNtt src;
+    int src_poly0 = -1;
 };
 
 // Number of source limbs of digit d (decomposeAndSplit's p0idxed - p0idxst,
@@ -170,8 +174,9 @@ __global__ void __launch_bounds__(kThreads) ntt_inv_tile(NttArgs a) {
     const uint64_t q = md.q;
     const int N = 1 << a.logN;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
+    const uint64_t *rd = a.src_poly0 >= 0 ? a.src.poly(a.src_poly0 + poly) + (long long)l * N : data;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < N; idx += kThreads) s[idx] = data[idx];
+    for (int idx = tid; idx < N; idx += kThreads) s[idx] = rd[idx];
     __syncthreads();
     const Tw *tw = a.tw1 + (size_t)m * N;
     for (int st = a.logN - 1; st >= 0; --st) {
@@ -857,9 +862,10 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
         // k*T + t); no block-wide barrier
         const long long rowoff = (long long)(blockIdx.x * C + c) * S;
         const bool fp = md.q < kFp64Bound;
+        const uint64_t *rd = a.src_poly0 >= 0 ? a.src.poly(a.src_poly0 + poly) + (long long)l * N : data;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint64_t x = data[MKF_DIDX(rowoff + k * T + t, N, kDbgNtt | 5)];
+            const uint64_t x = rd[MKF_DIDX(rowoff + k * T + t, N, kDbgNtt | 5)];
             s[(sb0 ^ swz(k * T))] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
         }
         __syncwarp();
@@ -936,10 +942,11 @@ static void launch_phases(const NttArgs &b, int np, int limbs, cudaStream_t st, 
 }
 
 static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st,
-                         bool inverse) {
+                         bool inverse, const OwnNtt *src = nullptr) {
     if (npolys <= 0 || ls.limbs <= 0) return;
     NttArgs a;
     a.ls = ls;
+    if (src) a.src = *src;
     a.mods = c.d_mods;
     a.logN = c.logN;
     a.n1 = c.n1;
@@ -954,6 +961,7 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
         int np = std::min(max_polys, npolys - p0);
         NttArgs b = a;
         b.ls.base = ls.base + (long long)p0 * ls.poly_stride;
+        if (src) b.src_poly0 = p0;
         dim3 block(kThreads);
         const double bytes = 16.0 * c.N * ls.limbs * np;
         if (c.n2 == 0) {
@@ -1270,6 +1278,10 @@ void ntt_forward(const Context &c, const LimbSet &ls, int npolys, cudaStream_t s
 }
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st) {
     launch_split(c, ls, npolys, st, true);
+}
+void ntt_inverse_from(const Context &c, const OwnNtt &src, const LimbSet &ls, int npolys,
+                      cudaStream_t st) {
+    launch_split(c, ls, npolys, st, true, &src);
 }
 
 } // namespace mkf

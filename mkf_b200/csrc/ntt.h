@@ -71,6 +71,10 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src, uint64_t *dig,
 void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, int npolys,
                         cudaStream_t st);
 void ntt_inverse(const Context &c, const LimbSet &ls, int npolys, cudaStream_t st);
+// Inverse NTT out of place: polynomial i < npolys is read from src.poly(i)
+// (same limbs and moduli as ls) and its transform is written to ls.
+void ntt_inverse_from(const Context &c, const OwnNtt &src, const LimbSet &ls, int npolys,
+                      cudaStream_t st);
 // Sets the kernels' launch attributes for c's device (idempotent); called
 // before a stream capture so that nothing but launches happens inside it.
 void ntt_prepare(const Context &c);
