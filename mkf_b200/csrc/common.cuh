@@ -118,6 +118,39 @@ template <typename I> MKF_DEV I dbg_idx(I v, unsigned long long bound, unsigned 
     do {                                                                                           \
     } while (0)
 #endif
+// Programmatic dependent launch.  The library's kernels are launched with
+// programmatic stream serialization (PdlLaunch below), so a kernel's blocks
+// may be scheduled while the previous kernel on the stream drains.  Every
+// such kernel first waits for the previous grid to complete (its writes are
+// then visible), and only then lets the next kernel be scheduled; the next
+// grid therefore launches once all of this grid's blocks have started, and
+// its blocks take the SMs this grid's last wave leaves free.
+MKF_DEV void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+struct PdlLaunch {
+    dim3 g, b;
+    size_t smem;
+    cudaStream_t st;
+    PdlLaunch(dim3 grid, dim3 block, size_t shared, cudaStream_t stream)
+        : g(grid), b(block), smem(shared), st(stream) {}
+    template <typename... KArgs, typename... Args>
+    void operator()(void (*kernel)(KArgs...), Args... args) const {
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = g;
+        cfg.blockDim = b;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    }
+};
+
 // Check tags: the translation unit in the high byte, the site below it.
 enum : unsigned {
     kDbgNtt = 0x01000000u, kDbgKernels = 0x02000000u, kDbgCanary = 0x0C000000u

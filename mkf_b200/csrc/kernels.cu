@@ -34,6 +34,7 @@ struct DecompArgs {
 };
 
 __global__ void __launch_bounds__(kBlock) decompose_kernel(DecompArgs a) {
+    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.N) return;
     const int d = a.digit0 + blockIdx.y;
@@ -103,7 +104,7 @@ void launch_decompose(const Context &c, const uint64_t *in, long long in_pstride
     ProfScope ps(c, PK_DECOMPOSE, st,
                  8.0 * c.N * npolys * ndigits * (a.alpha + level + 1 + c.nP));
     note_launch();
-    decompose_kernel<<<grid_for(c.N, ndigits, npolys), kBlock, 0, st>>>(a);
+    PdlLaunch(grid_for(c.N, ndigits, npolys), kBlock, 0, st)(decompose_kernel, a);
 }
 
 // y_i and the float64 correction of every (poly, digit, coefficient)
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in,
                                                              const DevModulus *mods, uint64_t *y,
                                                              uint8_t *v, int level, int alpha,
                                                              int ndigits, int N, int n1, int n2) {
+    pdl_enter();
     __shared__ uint64_t tile[2][32][33]; // double-buffered: one barrier per limb
     __shared__ uint8_t vt[32][33];
     const int d = blockIdx.y, p = blockIdx.z;
@@ -195,7 +197,7 @@ void decompose_ntt(const Context &c, const uint64_t *in, long long in_pstride, i
     if (!ring_r && alpha >= 2) {
         ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
         note_launch();
-        digits_prep_kernel<<<dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st>>>(
+        PdlLaunch(dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st)(digits_prep_kernel, 
             in, in_pstride, c.d_decomp[gamma - 1], c.d_mods, y, v, level, alpha, ndigits, c.N,
             c.n1, c.n2);
     }
@@ -225,7 +227,7 @@ bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride
     if (alpha >= 2) {
         ProfScope ps(c, PK_DECOMPOSE, st, 8.0 * c.N * npolys * ndigits * (2.0 * alpha) + n);
         note_launch();
-        digits_prep_kernel<<<dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st>>>(
+        PdlLaunch(dim3(c.N / 1024, ndigits, npolys), kBlock, 0, st)(digits_prep_kernel, 
             in, in_pstride, c.d_decomp[0], c.d_mods, y, v, level, alpha, ndigits, c.N, c.n1,
             c.n2);
     }
@@ -252,6 +254,7 @@ bool decompose_ntt_ip(const Context &c, const uint64_t *in, long long in_pstride
 template <int NIN, int NOUT, int W>
 __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mods, int N,
                                                      int pmod0) {
+    pdl_enter();
     const int x = (blockIdx.x * blockDim.x + threadIdx.x) * W;
     if (x >= N) return;
     const int l = blockIdx.y, g = blockIdx.z;
@@ -346,13 +349,13 @@ static void launch_ip_w(const Context &c, const IpArgs &a, cudaStream_t st) {
     dim3 grid((c.N / W + blk - 1) / blk, a.L1 + a.nP, a.groups);
     const int pm = c.pidx(0);
     if (a.nin == 1 && a.nout == 1)
-        ip_kernel<1, 1, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+        PdlLaunch(grid, blk, 0, st)(ip_kernel<1, 1, W>, a, c.d_mods, c.N, pm);
     else if (a.nin == 1 && a.nout == 2)
-        ip_kernel<1, 2, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+        PdlLaunch(grid, blk, 0, st)(ip_kernel<1, 2, W>, a, c.d_mods, c.N, pm);
     else if (a.nin == 2 && a.nout == 2)
-        ip_kernel<2, 2, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+        PdlLaunch(grid, blk, 0, st)(ip_kernel<2, 2, W>, a, c.d_mods, c.N, pm);
     else if (a.nin == 2 && a.nout == 1)
-        ip_kernel<2, 1, W><<<grid, blk, 0, st>>>(a, c.d_mods, c.N, pm);
+        PdlLaunch(grid, blk, 0, st)(ip_kernel<2, 1, W>, a, c.d_mods, c.N, pm);
 }
 
 void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
@@ -387,6 +390,7 @@ struct ModUpArgs {
 
 template <int MAXNS>
 __global__ void __launch_bounds__(kBlock) modup_kernel(ModUpArgs a) {
+    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.N) return;
     const uint64_t *src = a.src + (long long)blockIdx.y * a.src_pstride;
@@ -414,15 +418,15 @@ void launch_modup(const Context &c, const ModUpTab &tab, const uint64_t *src, lo
     dim3 grid = grid_for(c.N, npolys);
     note_launch();
     if (tab.ns <= 4)
-        modup_kernel<4><<<grid, kBlock, 0, st>>>(a);
+        PdlLaunch(grid, kBlock, 0, st)(modup_kernel<4>, a);
     else if (tab.ns <= 8)
-        modup_kernel<8><<<grid, kBlock, 0, st>>>(a);
+        PdlLaunch(grid, kBlock, 0, st)(modup_kernel<8>, a);
     else if (tab.ns <= 16)
-        modup_kernel<16><<<grid, kBlock, 0, st>>>(a);
+        PdlLaunch(grid, kBlock, 0, st)(modup_kernel<16>, a);
     else if (tab.ns <= 32)
-        modup_kernel<32><<<grid, kBlock, 0, st>>>(a);
+        PdlLaunch(grid, kBlock, 0, st)(modup_kernel<32>, a);
     else
-        modup_kernel<64><<<grid, kBlock, 0, st>>>(a);
+        PdlLaunch(grid, kBlock, 0, st)(modup_kernel<64>, a);
 }
 
 // Summed ModUp: out = sum over terms of ModUp(term) mod p, canonical.  Every
@@ -445,6 +449,7 @@ struct ModUpSumArgs {
 
 template <int MAXNS>
 __global__ void __launch_bounds__(kBlock) modup_sum_kernel(ModUpSumArgs a, int ch) {
+    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.N) return;
     const int p = blockIdx.y / a.nchunks, j0 = (blockIdx.y % a.nchunks) * ch;
@@ -506,15 +511,15 @@ void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src
     const dim3 grid = grid_for(c.N, npolys * nchunks);
     note_launch();
     if (tab.ns <= 4)
-        modup_sum_kernel<4><<<grid, kBlock, 0, st>>>(a, ch);
+        PdlLaunch(grid, kBlock, 0, st)(modup_sum_kernel<4>, a, ch);
     else if (tab.ns <= 8)
-        modup_sum_kernel<8><<<grid, kBlock, 0, st>>>(a, ch);
+        PdlLaunch(grid, kBlock, 0, st)(modup_sum_kernel<8>, a, ch);
     else if (tab.ns <= 16)
-        modup_sum_kernel<16><<<grid, kBlock, 0, st>>>(a, ch);
+        PdlLaunch(grid, kBlock, 0, st)(modup_sum_kernel<16>, a, ch);
     else if (tab.ns <= 32)
-        modup_sum_kernel<32><<<grid, kBlock, 0, st>>>(a, ch);
+        PdlLaunch(grid, kBlock, 0, st)(modup_sum_kernel<32>, a, ch);
     else
-        modup_sum_kernel<64><<<grid, kBlock, 0, st>>>(a, ch);
+        PdlLaunch(grid, kBlock, 0, st)(modup_sum_kernel<64>, a, ch);
 }
 
 // ----------------------------------------------------------------------------
@@ -522,6 +527,7 @@ void launch_modup_sum(const Context &c, const ModUpTab &tab, const uint64_t *src
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) moddown_combine_kernel(CombineSpec a, ModMap mm,
                                                                   const DevModulus *mods, int N) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, p = blockIdx.z;
@@ -552,7 +558,7 @@ void launch_moddown_combine(const Context &c, const CombineSpec &s, int nl, ModM
     ProfScope ps(c, PK_COMBINE, st,
                  8.0 * c.N * nl * npolys * ((s.x ? 2.0 : 1.0) * s.terms + 1 + (s.accumulate ? 1 : 0)));
     note_launch();
-    moddown_combine_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(s, mm, c.d_mods, c.N);
+    PdlLaunch(grid_for(c.N, nl, npolys), kBlock, 0, st)(moddown_combine_kernel, s, mm, c.d_mods, c.N);
 }
 
 // ----------------------------------------------------------------------------
@@ -565,6 +571,7 @@ MKF_DEV uint64_t mulmod_dev(uint64_t a, uint64_t b, const DevModulus &m) {
 __global__ void karatsuba_kernel(const uint64_t *a0, const uint64_t *a1, const uint64_t *b0,
                                  const uint64_t *b1, uint64_t *mu0, uint64_t *mu1, uint64_t *mu2,
                                  const DevModulus *mods, ModMap mm, int N) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y;
@@ -584,13 +591,14 @@ void launch_karatsuba(const Context &c, const uint64_t *a0, const uint64_t *a1, 
                       ModMap mm, cudaStream_t st) {
     ProfScope ps(c, PK_TENSOR, st, 8.0 * c.N * nl * 7);
     note_launch();
-    karatsuba_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(a0, a1, b0, b1, mu0, mu1, mu2, c.d_mods,
+    PdlLaunch(grid_for(c.N, nl), kBlock, 0, st)(karatsuba_kernel, a0, a1, b0, b1, mu0, mu1, mu2, c.d_mods,
                                                             mm, c.N);
 }
 
 __global__ void kklss_tensor_kernel(const uint64_t *a, const uint64_t *b, uint64_t *out,
                                     const unsigned char *has0, const unsigned char *has1,
                                     const DevModulus *mods, ModMap mm, int N, long long cs) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, j = blockIdx.z; // component j in [0, k]
@@ -613,7 +621,7 @@ void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b,
                          ModMap mm, long long comp_stride, cudaStream_t st) {
     ProfScope ps(c, PK_TENSOR, st, 8.0 * c.N * nl * 3.0 * (k + 1));
     note_launch();
-    kklss_tensor_kernel<<<grid_for(c.N, nl, k + 1), kBlock, 0, st>>>(a, b, out, d_has0, d_has1,
+    PdlLaunch(grid_for(c.N, nl, k + 1), kBlock, 0, st)(kklss_tensor_kernel, a, b, out, d_has0, d_has1,
                                                                       c.d_mods, mm, c.N,
                                                                       comp_stride);
 }
@@ -621,6 +629,7 @@ void launch_kklss_tensor(const Context &c, const uint64_t *a, const uint64_t *b,
 __global__ void mul_const_kernel(const uint64_t *x, long long xps, const uint64_t *cst,
                                  uint64_t *out, long long ops, const DevModulus *mods, ModMap mm,
                                  int N) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, p = blockIdx.z;
@@ -634,12 +643,13 @@ void launch_mul_const(const Context &c, const uint64_t *x, long long x_pstride,
                       ModMap mm, int npolys, cudaStream_t st) {
     ProfScope ps(c, PK_ELEMENTWISE, st, 16.0 * c.N * nl * npolys);
     note_launch();
-    mul_const_kernel<<<grid_for(c.N, nl, npolys), kBlock, 0, st>>>(x, x_pstride, mform_const, out,
+    PdlLaunch(grid_for(c.N, nl, npolys), kBlock, 0, st)(mul_const_kernel, x, x_pstride, mform_const, out,
                                                                    out_pstride, c.d_mods, mm, c.N);
 }
 
 __global__ void add_kernel(uint64_t *acc, const uint64_t *x, const DevModulus *mods, ModMap mm,
                            int N) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y;
@@ -652,7 +662,7 @@ void launch_add(const Context &c, uint64_t *acc, const uint64_t *x, int nl, ModM
                 cudaStream_t st) {
     ProfScope ps(c, PK_ELEMENTWISE, st, 24.0 * c.N * nl);
     note_launch();
-    add_kernel<<<grid_for(c.N, nl), kBlock, 0, st>>>(acc, x, c.d_mods, mm, c.N);
+    PdlLaunch(grid_for(c.N, nl), kBlock, 0, st)(add_kernel, acc, x, c.d_mods, mm, c.N);
 }
 
 // out_c = a_c (op) b_c over ncomp components of nl limbs (b_cs = 0: one b
@@ -662,6 +672,7 @@ __global__ void ew_binary_kernel(const uint64_t *a, long long a_cs, const uint64
                                  long long b_cs, uint64_t *out, long long out_cs,
                                  const DevModulus *mods, ModMap mm, int N, int op,
                                  EwFactors f) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, cidx = blockIdx.z;
@@ -689,7 +700,7 @@ void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const
     ProfScope ps(c, PK_ELEMENTWISE, st, 8.0 * c.N * nl * (2.0 * ncomp + (b_cs ? ncomp : 1)));
     note_launch();
     EwFactors none;
-    ew_binary_kernel<<<grid_for(c.N, nl, ncomp), kBlock, 0, st>>>(a, a_cs, b, b_cs, out, out_cs,
+    PdlLaunch(grid_for(c.N, nl, ncomp), kBlock, 0, st)(ew_binary_kernel, a, a_cs, b, b_cs, out, out_cs,
                                                                   c.d_mods, mm, c.N, op,
                                                                   f ? *f : none);
 }
@@ -704,6 +715,7 @@ void launch_ew_binary(const Context &c, const uint64_t *a, long long a_cs, const
 __global__ void slot_const_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
                                   long long out_cs, SlotConsts sc, const DevModulus *mods, int N,
                                   int mode) {
+    pdl_enter();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
     const int l = blockIdx.y, u = blockIdx.z;
@@ -726,7 +738,7 @@ void launch_slot_const(const Context &c, const uint64_t *in, long long in_cs, ui
     if (ncomp <= 0 || nl <= 0) return;
     ProfScope ps(c, PK_ELEMENTWISE, st, 8.0 * c.N * nl * ncomp * (mode == kSlotMulAdd ? 3 : 2));
     note_launch();
-    slot_const_kernel<<<grid_for(c.N, nl, ncomp), kBlock, 0, st>>>(in, in_cs, out, out_cs, sc,
+    PdlLaunch(grid_for(c.N, nl, ncomp), kBlock, 0, st)(slot_const_kernel, in, in_cs, out, out_cs, sc,
                                                                    c.d_mods, c.N, mode);
 }
 
@@ -738,6 +750,7 @@ void launch_slot_const(const Context &c, const uint64_t *in, long long in_cs, ui
 __global__ void automorphism_coeff_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
                                           long long out_cs, const DevModulus *mods, int N, int logN,
                                           uint64_t g) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int l = blockIdx.y, cidx = blockIdx.z;
@@ -752,6 +765,7 @@ __global__ void automorphism_coeff_kernel(const uint64_t *in, long long in_cs, u
 // a at the slot whose exponent is (2 brev(j) + 1) g mod 2N -- a gather.
 __global__ void automorphism_ntt_kernel(const uint64_t *in, long long in_cs, uint64_t *out,
                                         long long out_cs, int N, int logN, uint64_t g) {
+    pdl_enter();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
     const int l = blockIdx.y, cidx = blockIdx.z;
@@ -769,9 +783,9 @@ void launch_automorphism(const Context &c, const uint64_t *in, long long in_cs, 
     note_launch();
     const dim3 grid = grid_for(c.N, nl, ncomp);
     if (ntt)
-        automorphism_ntt_kernel<<<grid, kBlock, 0, st>>>(in, in_cs, out, out_cs, c.N, c.logN, galois);
+        PdlLaunch(grid, kBlock, 0, st)(automorphism_ntt_kernel, in, in_cs, out, out_cs, c.N, c.logN, galois);
     else
-        automorphism_coeff_kernel<<<grid, kBlock, 0, st>>>(in, in_cs, out, out_cs, c.d_mods, c.N,
+        PdlLaunch(grid, kBlock, 0, st)(automorphism_coeff_kernel, in, in_cs, out, out_cs, c.d_mods, c.N,
                                                            c.logN, galois);
 }
 
@@ -780,6 +794,7 @@ void launch_automorphism(const Context &c, const uint64_t *in, long long in_cs, 
 // ----------------------------------------------------------------------------
 __global__ void rescale_spread_kernel(const uint64_t *xL, long long xls, int L, uint64_t *t,
                                       long long ts, const DevModulus *mods, int N) {
+    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= N) return;
     const int i = blockIdx.y, p = blockIdx.z;
@@ -797,13 +812,14 @@ void launch_rescale_spread(const Context &c, const uint64_t *xL, long long xl_ps
                            uint64_t *t, long long t_pstride, int npolys, cudaStream_t st) {
     ProfScope ps(c, PK_RESCALE, st, 8.0 * c.N * npolys * (L + 1));
     note_launch();
-    rescale_spread_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(xL, xl_pstride, L, t,
+    PdlLaunch(grid_for(c.N, L, npolys), kBlock, 0, st)(rescale_spread_kernel, xL, xl_pstride, L, t,
                                                                       t_pstride, c.d_mods, c.N);
 }
 
 __global__ void rescale_combine_kernel(const uint64_t *in, long long ins, const uint64_t *t,
                                        long long ts, const uint64_t *rs, int L, uint64_t *out,
                                        long long os, const DevModulus *mods, int N, int nQ) {
+    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= N) return;
     const int i = blockIdx.y, p = blockIdx.z;
@@ -819,12 +835,13 @@ void launch_rescale_combine(const Context &c, const uint64_t *in, long long in_p
                             long long out_pstride, int npolys, cudaStream_t st) {
     ProfScope ps(c, PK_RESCALE, st, 24.0 * c.N * npolys * L);
     note_launch();
-    rescale_combine_kernel<<<grid_for(c.N, L, npolys), kBlock, 0, st>>>(
+    PdlLaunch(grid_for(c.N, L, npolys), kBlock, 0, st)(rescale_combine_kernel, 
         in, in_pstride, t, t_pstride, c.d_rescale, L, out, out_pstride, c.d_mods, c.N, c.nQ);
 }
 
 __global__ void replicate_kernel(const uint64_t *src, uint64_t *dst, long long words, int ncopies,
                                  long long ds) {
+    pdl_enter();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= words) return;
     const uint64_t v = src[i];
@@ -835,7 +852,7 @@ void launch_replicate(const uint64_t *src, uint64_t *dst, long long words, int n
                       long long dst_stride, cudaStream_t st) {
     if (words <= 0 || ncopies <= 0) return;
     note_launch();
-    replicate_kernel<<<(unsigned)((words + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+    PdlLaunch((unsigned)((words + kBlock - 1) / kBlock), kBlock, 0, st)(replicate_kernel, 
         src, dst, words, ncopies, dst_stride);
 }
 

@@ -142,6 +142,7 @@ constexpr unsigned mask(int LOGS, int in16, bool cols, int out16) {
 // logN <= 12: a whole limb of N <= 4096 words in one tile, one stage per
 // barrier (Harvey butterflies; outputs canonical).
 __global__ void __launch_bounds__(kThreads) ntt_fwd_tile(NttArgs a) {
+    pdl_enter();
     __shared__ uint64_t s[kTile];
     const int poly = blockIdx.y / a.ls.limbs, l = blockIdx.y % a.ls.limbs;
     const int m = a.ls.mod_of(l);
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(kThreads) ntt_fwd_tile(NttArgs a) {
 }
 
 __global__ void __launch_bounds__(kThreads) ntt_inv_tile(NttArgs a) {
+    pdl_enter();
     __shared__ uint64_t s[kTile];
     const int poly = blockIdx.y / a.ls.limbs, l = blockIdx.y % a.ls.limbs;
     const int m = a.ls.mod_of(l);
@@ -458,6 +460,7 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
 
 template <int LOGS, bool COLS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
+    pdl_enter();
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
     __shared__ uint64_t s[kTile];
     const int limbs = a.ls.limbs;
@@ -557,7 +560,7 @@ template <int LOGS, bool COLS>
 static void launch_fwd_phase(dim3 grid, cudaStream_t st, const NttArgs &b, int device) {
     constexpr size_t sm = fwd_phase_smem<LOGS, COLS>();
     smem_attr(ntt_fwd_phase<LOGS, COLS>, device, sm);
-    ntt_fwd_phase<LOGS, COLS><<<grid, kPhaseThreads, sm, st>>>(b);
+    PdlLaunch(grid, kPhaseThreads, sm, st)(ntt_fwd_phase<LOGS, COLS>, b);
 }
 
 MKF_DEV void cp_async16(void *smem, const void *gmem) {
@@ -589,6 +592,7 @@ constexpr size_t kColSmem = (size_t)kColWords * 8 * 2;
 
 template <int LOGS>
 __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
+    pdl_enter();
     constexpr int S = 1 << LOGS, T = S / 8, C = kColWords / S, NW = kColWords;
     extern __shared__ __align__(16) uint64_t dsm[];
     uint64_t *s = dsm;                 // exchange tile, C columns
@@ -844,6 +848,7 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
 
 template <int LOGS, bool COLS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
+    pdl_enter();
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
     __shared__ uint64_t s[kTile];
     const int limbs = a.ls.limbs;
@@ -927,10 +932,10 @@ static void launch_phases(const NttArgs &b, int np, int limbs, cudaStream_t st, 
     if (inverse) {
         {
             ProfScope ps(c, PK_NTT_INV_ROW, st, bytes);
-            ntt_inv_phase<LOG2, false><<<g2, block, 0, st>>>(b);
+            PdlLaunch(g2, block, 0, st)(ntt_inv_phase<LOG2, false>, b);
         }
         ProfScope ps(c, PK_NTT_INV_COL, st, bytes);
-        ntt_inv_phase<LOG1, true><<<g1, block, 0, st>>>(b);
+        PdlLaunch(g1, block, 0, st)(ntt_inv_phase<LOG1, true>, b);
     } else {
         {
             ProfScope ps(c, PK_NTT_FWD_COL, st, bytes);
@@ -969,9 +974,9 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
             ProfScope ps(c, inverse ? PK_NTT_INV_FULL : PK_NTT_FWD_FULL, st, bytes);
             note_launch();
             if (inverse)
-                ntt_inv_tile<<<grid, block, 0, st>>>(b);
+                PdlLaunch(grid, block, 0, st)(ntt_inv_tile, b);
             else
-                ntt_fwd_tile<<<grid, block, 0, st>>>(b);
+                PdlLaunch(grid, block, 0, st)(ntt_fwd_tile, b);
         } else {
             switch (c.logN) {
             case 13: launch_phases<6, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
@@ -999,6 +1004,7 @@ constexpr size_t kRowIpSmem = 3 * kTile * sizeof(uint64_t);
 // sum equals the stand-alone inner product's exactly.
 template <int LOGS>
 __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a, DigitIpArgs g) {
+    pdl_enter();
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
     extern __shared__ __align__(16) uint64_t dsm[];
     uint64_t *s = dsm;
@@ -1169,14 +1175,14 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
             dim3 g1((1 << L2G) / (kColWords >> L1G), npp, c.tune.col_split);                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col * npp / np);                              \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
-            ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
+            PdlLaunch(g1, kColThreads, kColSmem, st)(ntt_fwd_digits_col<L1G>, b, sb);                     \
             if (p0) note_launch(1);                                                                \
         }                                                                                          \
         dim3 g2((1 << L1G) / (kTile >> L2G) * ip.nin, limbs, ip.groups);                           \
         ProfScope ps(c, PK_DIGITS_ROW_IP, st, bytes_row);                                          \
         smem_attr(ntt_digits_row_ip<L2G>, c.device, kRowIpSmem);                                   \
         note_launch(1);                                                                            \
-        ntt_digits_row_ip<L2G><<<g2, block, kRowIpSmem, st>>>(a, ip);                              \
+        PdlLaunch(g2, block, kRowIpSmem, st)(ntt_digits_row_ip<L2G>, a, ip);                              \
         break;                                                                                     \
     }
         MKF_DIGITS_IP_CASE(13, 6, 7)
@@ -1250,7 +1256,7 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
             smem_attr(ntt_fwd_digits_col<L1G>, c.device, kColSmem);              \
-            ntt_fwd_digits_col<L1G><<<g1, kColThreads, kColSmem, st>>>(b, sb);                     \
+            PdlLaunch(g1, kColThreads, kColSmem, st)(ntt_fwd_digits_col<L1G>, b, sb);                     \
         }                                                                                          \
         ProfScope ps(c, PK_DIGITS_ROW, st, bytes_row);                                             \
         launch_fwd_phase<L2G, false>(g2, st, b, c.device);                                         \
