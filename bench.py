@@ -842,16 +842,17 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
     tried = {}
     best = None
     for lanes in [int(x) for x in a.lanes.split(",") if x]:
-        b = ev.Batch(P0, items, lanes=lanes, graph=True)
-        ms = timed(lambda: b.launch(cs), reps)
-        tried[lanes] = ms
-        if best is None or ms < best[1]:
-            if best is not None:
-                best[0].close()
-            best = (b, ms, lanes)
-        else:
-            b.close()
-    b, batch_ms, lanes = best
+        for fuse in (False, True):
+            b = ev.Batch(P0, items, lanes=lanes, graph=True, fuse_keys=fuse)
+            ms = timed(lambda: b.launch(cs), reps)
+            tried[f"{lanes}{' fused' if fuse else ''}"] = ms
+            if best is None or ms < best[1]:
+                if best is not None:
+                    best[0].close()
+                best = (b, ms, lanes, fuse)
+            else:
+                b.close()
+    b, batch_ms, lanes, fuse = best
     L.mkf_launch_count(1)
     batch_ms = timed(lambda: b.launch(cs), reps)
     kernels = int(L.mkf_launch_count(0)) // (reps + max(1, a.warmup))
@@ -869,7 +870,7 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
                     it[1].MulRelin(it[2], it[3], it[4], rescale=True, materialize=True, stream=cs)
 
             p_ms = timed(plain_sub, reps)
-            bb = ev.Batch(P0, sub, lanes=lanes, graph=True)
+            bb = ev.Batch(P0, sub, lanes=lanes, graph=True, fuse_keys=fuse)
             b_ms = timed(lambda: bb.launch(cs), reps)
             bb.close()
             buckets[f"{name}_k{kb}"] = {"products": len(sub), "plain_ms": p_ms, "batched_ms": b_ms,
@@ -880,9 +881,10 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
            "products": n,
            "plain": {"value": n / (plain_ms / 1e3), "unit": "mult+relin ops/s", "ms": plain_ms},
            "batched": {"value": n / (batch_ms / 1e3), "unit": "mult+relin ops/s", "ms": batch_ms,
-                       "lanes": lanes, "graph": True, "kernels_per_launch": kernels},
+                       "lanes": lanes, "graph": True, "fuse_keys": fuse,
+                       "kernels_per_launch": kernels},
            "batched_over_plain": plain_ms / batch_ms,
-           "autotune_lanes_ms": tried,
+           "autotune_plan_ms": tried,
            "buckets": buckets,
            "mix": {f"k{k}": sum(1 for s in shapes if s[1] == k) for k in (2, 4, 8, 16)}}
     b.close()
