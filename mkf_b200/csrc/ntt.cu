@@ -587,16 +587,16 @@ template <int NPEND> MKF_DEV void cp_async_wait() {
 // one, reduced from the source limb.  The integer multSum's 128-bit sum needs
 // no reduction on the way: its high word stays below ns * q_i * p_j / 2^64.
 constexpr int kColThreads = 256, kColWords = 2048;
-// dynamic shared memory: the exchange tile and one staged source limb
-constexpr size_t kColSmem = (size_t)kColWords * 8 * 2;
+// dynamic shared memory: two exchange tiles (alternating limbs) and one
+// staged source limb
+constexpr size_t kColSmem = (size_t)kColWords * 8 * 3;
 
 template <int LOGS>
 __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
     pdl_enter();
     constexpr int S = 1 << LOGS, T = S / 8, C = kColWords / S, NW = kColWords;
     extern __shared__ __align__(16) uint64_t dsm[];
-    uint64_t *s = dsm;                 // exchange tile, C columns
-    uint64_t *ys = dsm + NW;           // [C][S] the staged one-limb source
+    uint64_t *ys = dsm + 2 * NW;       // [C][S] the staged one-limb source
     const int limbs = a.ls.limbs;
     const int pd = blockIdx.y, poly = pd / src.ndigits, d = pd % src.ndigits;
     const int N = 1 << a.logN, R = 1 << a.n2;
@@ -630,6 +630,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
     // of the last wave)
     const int per = (limbs + gridDim.z - 1) / gridDim.z;
     const int l_end = min(limbs, (int)(blockIdx.z + 1) * per);
+    int buf = 0;
     for (int l = blockIdx.z * per; l < l_end; ++l) {
         const bool own_limb = l < L1 && l >= start && l < start + ns;
         uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
@@ -646,6 +647,12 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             }
             continue;
         }
+        // exchange tile of this limb: the two tiles alternate over the limbs
+        // that use one, so the barrier before a limb's row-major store also
+        // orders the store of the limb before it against this limb's passes
+        // (one barrier per limb)
+        uint64_t *s = dsm + buf * NW;
+        buf ^= 1;
         const int m = a.ls.mod_of(l);
         const DevModulus md = a.mods[m];
         const uint64_t q = md.q;
@@ -751,7 +758,6 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             const int r = idx / C, cc = idx % C;
             dst[(long long)r * R + cc] = s[saddr<S>(cc, r)];
         }
-        __syncthreads();
     }
 }
 
