@@ -101,7 +101,10 @@ enum {
 };
 /* Words a key of `kind` occupies at full level. */
 size_t mkf_key_words(const mkf_ctx *ctx, int kind);
-/* Uploads key words from host memory into HBM. */
+/* Uploads key words from host memory into HBM.  A switching key's limbs
+ * whose modulus is below 2^50 are kept in HBM as the bits of their centered
+ * doubles (w or w - q, |.| <= q/2), the form the float64 inner products
+ * multiply with; the words passed in and their meaning are the same. */
 mkf_status mkf_key_upload(mkf_ctx *ctx, int kind, const uint64_t *words, size_t n_words,
                           mkf_key **out);
 void mkf_key_destroy(mkf_key *key);

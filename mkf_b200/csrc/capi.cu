@@ -468,6 +468,16 @@ mkf_status mkf_key_upload(mkf_ctx *ctx, int kind, const uint64_t *words, size_t 
         delete k;
         return fail(ctx, MKF_ERR_CUDA, "key upload failed");
     }
+    if (kind == MKF_KEY_SWITCHING) {
+        // float64 limbs held as centered doubles (what the inner products read)
+        launch_key_to_f64(ctx->c, k->d, (int)(need / ((size_t)(ctx->c.nQ + ctx->c.nP) * ctx->c.N)),
+                          nullptr);
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(k->d);
+            delete k;
+            return fail(ctx, MKF_ERR_CUDA, "key conversion failed");
+        }
+    }
     *out = k;
     return MKF_OK;
 }

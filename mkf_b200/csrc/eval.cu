@@ -189,6 +189,7 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     ip.a_gstride = beta * qp;
     ip.a_istride = kk * beta * qp;
     ip.use_bptr = 1;
+    ip.b_f64 = 1;
     for (int i = 0; i < k; ++i) ip.bptr[i] = fold.p[i];
     ip.b_tstride = 2LL * (nQ + nP) * N;
     ip.b_ostride = (long long)(nQ + nP) * N;
@@ -412,6 +413,7 @@ std::string mkf_ckks_mulrelin_multi(const Context &c, Arena &ar, cudaStream_t st
         r.a_tstride = qp;
         r.a_gstride = beta * qp;
         r.B = relin;
+        r.b_f64 = 1;
         r.b_tstride = 2LL * (nQ + nP) * N;
         r.b_ostride = (long long)(nQ + nP) * N;
         r.b_qlimbs = nQ;
@@ -586,6 +588,7 @@ std::string mkf_mulrelin(const Context &c, Arena &ar, cudaStream_t st, int schem
         r.A = rdig;
         r.a_tstride = qp;
         r.B = relin;
+        r.b_f64 = 1;
         r.b_tstride = 2LL * (nQ + nP) * N;
         r.b_ostride = (long long)(nQ + nP) * N;
         r.b_qlimbs = nQ;

@@ -267,6 +267,7 @@ __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mod
     const long long boff = (a.use_bptr && !a.bptr_per_term ? 0 : (long long)g * a.b_gstride) + blimb;
     const uint64_t *Bg = a.use_bptr && !a.bptr_per_term ? a.bptr[MKF_DIDX(g, 64, kDbgKernels | 1)] : a.B;
     MKF_DCHECK_LT(l, a.L1 + a.nP, kDbgKernels | 2);
+    const bool bf = a.b_f64 && m.q < kFp64Bound;
     MKF_DCHECK_LT(a.nterms, a.bptr_per_term ? 65 : 1 << 20, kDbgKernels | 3);
     Acc128 acc[NIN][NOUT][W];
 #pragma unroll
@@ -290,7 +291,13 @@ __global__ void __launch_bounds__(512) ip_kernel(IpArgs a, const DevModulus *mod
         const uint64_t *bp = (a.bptr_per_term ? a.bptr[MKF_DIDX(t, 64, kDbgKernels | 3)] : Bg) + boff +
                              (a.bptr_per_term ? 0 : (long long)t * a.b_tstride);
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) ldw(bp + (long long)o * a.b_ostride, bv[o]);
+        for (int o = 0; o < NOUT; ++o) {
+            ldw(bp + (long long)o * a.b_ostride, bv[o]);
+            if (bf) {
+#pragma unroll
+                for (int w = 0; w < W; ++w) bv[o][w] = canon_f(__longlong_as_double((long long)bv[o][w]), m.qd);
+            }
+        }
 #pragma unroll
         for (int i = 0; i < NIN; ++i)
             ldw(a.A + aoff + (long long)i * a.a_istride + (long long)t * a.a_tstride, av[i]);
@@ -372,6 +379,27 @@ void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st) {
         launch_ip_w<2>(c, a, st);
     else
         launch_ip_w<1>(c, a, st);
+}
+
+// Switching keys in HBM: limbs below 2^50 are held as the bits of their
+// centered doubles, the form the float64 inner products multiply with, so
+// no product converts a key word again.  words: [beta][2][nQ+nP][N].
+__global__ void __launch_bounds__(kBlock) key_to_f64_kernel(uint64_t *words, const DevModulus *mods,
+                                                            int N, int nQ, int nP, int pmod0) {
+    pdl_enter();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    const int l = blockIdx.y, poly = blockIdx.z;
+    const DevModulus m = mods[l < nQ ? l : pmod0 + (l - nQ)];
+    if (m.q >= kFp64Bound) return;
+    uint64_t *w = words + ((long long)poly * (nQ + nP) + l) * N + x;
+    *w = (uint64_t)__double_as_longlong(centered_f(*w % m.q, m.q));
+}
+
+void launch_key_to_f64(const Context &c, uint64_t *words, int npolys, cudaStream_t st) {
+    note_launch();
+    PdlLaunch(grid_for(c.N, c.nQ + c.nP, npolys), kBlock, 0, st)(key_to_f64_kernel, words, c.d_mods,
+                                                                 c.N, c.nQ, c.nP, c.pidx(0));
 }
 
 // ----------------------------------------------------------------------------

@@ -62,12 +62,18 @@ struct IpArgs {
     int nterms = 0, nin = 1, nout = 1, groups = 1;
     int L1 = 0, nP = 0;
     int mform_out = 0, accumulate = 0;
+    // B is a switching key as mkf_key_upload stores it: limbs below 2^50 hold
+    // centered doubles (converted back to canonical words on load)
+    int b_f64 = 0;
     // optional per-group (or, with bptr_per_term, per-term) B base pointers,
     // passed by value so that no table has to be uploaded per call
     int use_bptr = 0, bptr_per_term = 0;
     const uint64_t *bptr[kMaxParties] = {};
 };
 void launch_ip(const Context &c, const IpArgs &a, cudaStream_t st);
+// Converts the limbs below 2^50 of npolys key polynomials ([npolys][nQ+nP][N],
+// canonical words) to the bits of their centered doubles, in place.
+void launch_key_to_f64(const Context &c, uint64_t *words, int npolys, cudaStream_t st);
 
 // Exact basis extension (modUpExact, basis_extension.go:337-357) of npolys
 // polynomials: tab.ns source limbs at src (+p*src_pstride, limb i at i*N) to

@@ -1072,8 +1072,11 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
             const bool red = (d & 3) == 3;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                double x0 = __dadd_rn(f0[k * T], mulvar_f(v[k], centered_f(__ldg(k0 + k * T), q), md.qd, md.qinvd));
-                double x1 = __dadd_rn(f1[k * T], mulvar_f(v[k], centered_f(__ldg(k1 + k * T), q), md.qd, md.qinvd));
+                // keys are stored as centered doubles on float64 limbs
+                double x0 = __dadd_rn(f0[k * T], mulvar_f(v[k], __longlong_as_double((long long)__ldg(k0 + k * T)),
+                                                          md.qd, md.qinvd));
+                double x1 = __dadd_rn(f1[k * T], mulvar_f(v[k], __longlong_as_double((long long)__ldg(k1 + k * T)),
+                                                          md.qd, md.qinvd));
                 if (red) {
                     x0 = reduce_f(x0, md.qinvd, md.qd);
                     x1 = reduce_f(x1, md.qinvd, md.qd);
