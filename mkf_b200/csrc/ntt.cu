@@ -754,9 +754,20 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
         }
         // the tile holds every column of the block: store it row-major
         __syncthreads();
-        for (int idx = tid; idx < NW; idx += kColThreads) {
-            const int r = idx / C, cc = idx % C;
-            dst[(long long)r * R + cc] = s[saddr<S>(cc, r)];
+        {
+            // element e of this thread is point e*RS + tid/C of column tid%C:
+            // its tile address is the thread's base XOR a constant and its
+            // destination the thread's base plus a constant.  The bases are
+            // formed from an opaque copy of tid each limb, so that they are
+            // not held in registers across the limb walk.
+            constexpr int RS = kColThreads / C;
+            static_assert(NW / kColThreads == 8 && RS * C == kColThreads, "store schedule");
+            int otid;
+            asm volatile("mov.u32 %0, %1;" : "=r"(otid) : "r"(tid));
+            const int tb = saddr<S>(otid % C, otid / C);
+            uint64_t *db = dst + (long long)(otid / C) * R + otid % C;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) db[(long long)e * RS * R] = s[tb ^ swz(e * RS)];
         }
     }
 }
