@@ -489,28 +489,33 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         uint64_t v[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[r] = data[MKF_DIDX(rowoff + r * T + t, N, kDbgNtt | 5)];
-        // the last pass leaves the row in the warp's tile region; it is
-        // stored from there in point order (lane t: points k*T + t)
+        // the last pass stays in registers: lane t then holds points
+        // 8t..8t+7 of its row and stores them as four 16-byte words (every
+        // lane loaded its words before the first exchange, so the row can be
+        // overwritten in place)
+        ulonglong2 *out2 = reinterpret_cast<ulonglong2 *>(data + rowoff + 8 * t);
         if (fp) {
             double vf[8];
 #pragma unroll
             for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
             const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-            fwd_passes_f<LOGS, 32, 8, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+            fwd_passes_f<LOGS, 32, 8, true, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[(sb0 ^ swz(k * T))]), md.qd);
+            for (int j = 0; j < 4; ++j)
+                out2[j] = make_ulonglong2(canon_f(vf[2 * j], md.qd), canon_f(vf[2 * j + 1], md.qd));
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
-                fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, true, true, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    data[rowoff + k * T + t] = reduce_any(s[(sb0 ^ swz(k * T))], q, md.one_sh);
+                for (int j = 0; j < 4; ++j)
+                    out2[j] = make_ulonglong2(reduce_any(v[2 * j], q, md.one_sh),
+                                              reduce_any(v[2 * j + 1], q, md.one_sh));
             } else {
-                fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, false, true, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[(sb0 ^ swz(k * T))], q);
+                for (int j = 0; j < 4; ++j)
+                    out2[j] = make_ulonglong2(reduce4(v[2 * j], q), reduce4(v[2 * j + 1], q));
             }
         }
         return;
@@ -774,16 +779,22 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
 // phase, whose global stage 0 folds in N^-1 and leaves canonical values.
-template <int LOGS, bool COLS, bool LAZY>
-MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, int t) {
+// REGIN: the first pass (p = NP-1, points 8t..8t+7 of the thread's
+// sub-transform) takes its words from vin instead of the tile; KEEP: the last
+// pass (p = 0, points r*T + t, i.e. point order) leaves them in vout.
+template <int LOGS, bool COLS, bool LAZY, bool REGIN = false, bool KEEP = false>
+MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, int t,
+                        const uint64_t *vin = nullptr, uint64_t *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
+    static_assert(pass_pos<LOGS>(NP - 1) == 0, "the first inverse pass holds consecutive points");
     const uint64_t q = md.q;
     uint64_t v[8];
 #pragma unroll
     for (int p = NP - 1; p >= 0; --p) {
         const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)];
+        for (int r = 0; r < 8; ++r)
+            v[r] = (REGIN && p == NP - 1) ? vin[r] : s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)];
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -811,9 +822,14 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
                 }
             }
         }
+        if (KEEP && p == 0) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = v[r];
-        __syncwarp();
+            for (int r = 0; r < 8; ++r) vout[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = v[r];
+            __syncwarp();
+        }
     }
 }
 
@@ -823,8 +839,9 @@ MKF_DEV void inv_passes(uint64_t *s, const Tw *tw, const DevModulus &md, int c, 
 // Row phases take centered words (IN 1/2) and hand the column phase words
 // below 1.375q.
 constexpr int kInvRowIn16 = 8, kInvMid16 = 22;
-template <int LOGS, bool COLS>
-MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int c, int t) {
+template <int LOGS, bool COLS, bool REGIN = false, bool KEEP = false>
+MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int c, int t,
+                          const double *vin = nullptr, double *vout = nullptr) {
     constexpr int S = 1 << LOGS, NP = (LOGS + 2) / 3;
     constexpr unsigned RED = COLS ? gsched::mask(LOGS, kInvMid16, true, 0)
                                   : gsched::mask(LOGS, kInvRowIn16, false, kInvMid16);
@@ -834,7 +851,10 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
     for (int p = NP - 1; p >= 0; --p) {
         const int pb = saddr<S>(c, elem<LOGS>(p, t, 0));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)]);
+        for (int r = 0; r < 8; ++r)
+            v[r] = (REGIN && p == NP - 1)
+                       ? vin[r]
+                       : __longlong_as_double((long long)s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)]);
 #pragma unroll
         for (int u = 2; u >= 0; --u) {
             const int st = 3 * p + u;
@@ -857,9 +877,14 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
                 }
             }
         }
+        if (KEEP && p == 0) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
-        __syncwarp();
+            for (int r = 0; r < 8; ++r) vout[r] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) s[MKF_DIDX(pb ^ swz(r << pass_pos<LOGS>(p)), kTile, kDbgNtt | 3)] = (uint64_t)__double_as_longlong(v[r]);
+            __syncwarp();
+        }
     }
 }
 
@@ -885,28 +910,36 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
         const long long rowoff = (long long)(blockIdx.x * C + c) * S;
         const bool fp = md.q < kFp64Bound;
         const uint64_t *rd = a.src_poly0 >= 0 ? a.src.poly(a.src_poly0 + poly) + (long long)l * N : data;
+        // the first inverse pass holds points 8t..8t+7: lane t loads them as
+        // four 16-byte words straight into its registers
+        const ulonglong2 *in2 = reinterpret_cast<const ulonglong2 *>(rd + MKF_DIDX(rowoff + 8 * t, N, kDbgNtt | 5));
+        uint64_t w[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint64_t x = rd[MKF_DIDX(rowoff + k * T + t, N, kDbgNtt | 5)];
-            s[(sb0 ^ swz(k * T))] = fp ? (uint64_t)__double_as_longlong(centered_f(x, md.q)) : x;
+        for (int j = 0; j < 4; ++j) {
+            const ulonglong2 x = in2[j];
+            w[2 * j] = x.x;
+            w[2 * j + 1] = x.y;
         }
-        __syncwarp();
         if (fp) {
-            inv_passes_f<LOGS, false>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md, c, t);
+            double wf[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[(sb0 ^ swz(k * T))];
+            for (int r = 0; r < 8; ++r) wf[r] = centered_f(w[r], md.q);
+            // the last pass holds points k*T + t (point order): stored directly
+            inv_passes_f<LOGS, false, true, true>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md, c,
+                                                  t, wf, wf);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = (uint64_t)__double_as_longlong(wf[k]);
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
-                inv_passes<LOGS, false, true>(s, tw, md, c, t);
+                inv_passes<LOGS, false, true, true, true>(s, tw, md, c, t, w, w);
                 // the first phase hands the second one values below 2q
 #pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    data[rowoff + k * T + t] = reduce_2q(s[(sb0 ^ swz(k * T))], md.q, md.one_sh);
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce_2q(w[k], md.q, md.one_sh);
             } else {
-                inv_passes<LOGS, false, false>(s, tw, md, c, t);
+                inv_passes<LOGS, false, false, true, true>(s, tw, md, c, t, w, w);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = s[(sb0 ^ swz(k * T))];
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = w[k];
             }
         }
         return;
