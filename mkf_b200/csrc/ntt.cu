@@ -1092,72 +1092,48 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
         // sum times 2^-64 is MRed's sum.  Bounds (q < 2^50): NTT outputs
         // below 3.6q, keys below q/2, each product below 0.95q, the sums
         // below 0.5q + 4 * 0.95q.
-        // The last radix-8 pass stays in registers: thread t of row c then
-        // holds points 8t..8t+7, whose keys, own-limb words and outputs are
-        // 64 contiguous bytes (16-byte loads and stores), and the
-        // accumulator of its register k sits at k*T + t (no bank conflicts).
         double *f0 = reinterpret_cast<double *>(acc0), *f1 = reinterpret_cast<double *>(acc1);
-        const long long krow8 = krow - t + 8 * t;
         for (int d = 0; d < g.beta; ++d) {
-            __syncwarp(); // the previous digit's exchanges end before this digit's
             const int start = d * g.alpha;
             const bool own = g.own.p[0] && l < g.L1 && l >= start &&
                              l < start + digit_ns(g.level, g.alpha, d);
             double v[8];
             if (own) {
-                const ulonglong2 *xn = reinterpret_cast<const ulonglong2 *>(
-                    g.own.poly(poly) + (long long)l * N + rowoff + 8 * t);
+                const uint64_t *xn = g.own.poly(poly) + (long long)l * N + rowoff + t;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const ulonglong2 w = xn[j];
-                    v[2 * j] = centered_f(w.x, q);
-                    v[2 * j + 1] = centered_f(w.y, q);
-                }
+                for (int k = 0; k < 8; ++k) v[k] = centered_f(xn[k * T], q);
             } else {
                 const uint64_t *src = g.dig + (long long)(poly * g.beta + d) * g.dig_pstride + (long long)l * N + rowoff + t;
 #pragma unroll
                 for (int r = 0; r < 8; ++r) v[r] = __longlong_as_double((long long)src[r * T]);
-                fwd_passes_f<LOGS, 32, 64, true, false, true>(s, twd, md.qd, md.qinvd, c, t, v);
+                fwd_passes_f<LOGS, 32, 64, false, false, true>(s, twd, md.qd, md.qinvd, c, t, v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = __longlong_as_double((long long)s[(sb0 ^ swz(k * T))]);
             }
-            // keys are stored as centered doubles on float64 limbs
-            const double2 *k0 = reinterpret_cast<const double2 *>(kb + (long long)d * g.k_tstride + krow8);
-            const double2 *k1 = reinterpret_cast<const double2 *>(kb + (long long)d * g.k_tstride + g.k_ostride + krow8);
+            const uint64_t *k0 = kb + (long long)d * g.k_tstride + krow;
+            const uint64_t *k1 = k0 + g.k_ostride;
             // every fourth digit the sums go back to q/2 (more digits than six)
             const bool red = (d & 3) == 3;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double2 a0 = __ldg(k0 + j), a1 = __ldg(k1 + j);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int k = 2 * j + h;
-                    double x0 = __dadd_rn(f0[k * T], mulvar_f(v[k], h ? a0.y : a0.x, md.qd, md.qinvd));
-                    double x1 = __dadd_rn(f1[k * T], mulvar_f(v[k], h ? a1.y : a1.x, md.qd, md.qinvd));
-                    if (red) {
-                        x0 = reduce_f(x0, md.qinvd, md.qd);
-                        x1 = reduce_f(x1, md.qinvd, md.qd);
-                    }
-                    f0[k * T] = x0;
-                    f1[k * T] = x1;
+            for (int k = 0; k < 8; ++k) {
+                // keys are stored as centered doubles on float64 limbs
+                double x0 = __dadd_rn(f0[k * T], mulvar_f(v[k], __longlong_as_double((long long)__ldg(k0 + k * T)),
+                                                          md.qd, md.qinvd));
+                double x1 = __dadd_rn(f1[k * T], mulvar_f(v[k], __longlong_as_double((long long)__ldg(k1 + k * T)),
+                                                          md.qd, md.qinvd));
+                if (red) {
+                    x0 = reduce_f(x0, md.qinvd, md.qd);
+                    x1 = reduce_f(x1, md.qinvd, md.qd);
                 }
+                f0[k * T] = x0;
+                f1[k * T] = x1;
             }
         }
-        uint64_t *o0 = g.out + (long long)grp * g.out_gstride + (long long)sidx * g.out_istride +
-                       (long long)l * N + rowoff + 8 * t;
-        ulonglong2 *p0 = reinterpret_cast<ulonglong2 *>(o0);
-        ulonglong2 *p1 = reinterpret_cast<ulonglong2 *>(o0 + g.out_ostride);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            uint64_t r0[2], r1[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int k = 2 * j + h;
-                r0[h] = canon_f(mulmod_f(reduce_f(f0[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
-                r1[h] = canon_f(mulmod_f(reduce_f(f1[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
-            }
-            p0[j] = make_ulonglong2(r0[0], r0[1]);
-            p1[j] = make_ulonglong2(r1[0], r1[1]);
+        for (int k = 0; k < 8; ++k) {
+            acc0[k * T] = canon_f(mulmod_f(reduce_f(f0[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
+            acc1[k * T] = canon_f(mulmod_f(reduce_f(f1[k * T], md.qinvd, md.qd), md.r64d, md.r64q, md.qd), md.qd);
         }
-        return;
     } else {
         for (int d = 0; d < g.beta; ++d) {
             const int start = d * g.alpha;
