@@ -25,6 +25,7 @@ CASES = {
     # KKLSS-BFV on the serving rings (S15 is the C2 chain), full level
     "kklss_bfv_s14_k8": ("kklss", "bfv", "S14", 8, -1),
     "kklss_bfv_c2_k4": ("kklss", "bfv", "C2", 4, -1),
+    "kklss_bfv_s15_k8": ("kklss", "bfv", "S15", 8, -1),
     "kklss_bfv_s16_k8": ("kklss", "bfv", "S16", 8, -1),
 }
 

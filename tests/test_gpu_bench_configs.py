@@ -7,8 +7,8 @@ testbench compares: hardware/u55c/hls/tb/tb_par1_mkf_ckks.cpp:46-63):
   (software/mkf/mkf_cpu/ckks.go:102-166);
 * KKLSS-CKKS mult+relin+rescale at k = 8 on the serving rings of logN 14, 15
   and 16 (software/kklss/mkckks/evaluator.go:419-446);
-* KKLSS-BFV mult+relin at k = 8 on the logN 14 and 16 serving rings and at
-  k = 4 on the logN 15 chain of fifteen 58-bit primes
+* KKLSS-BFV mult+relin at k = 8 on the logN 14, 15 and 16 serving rings
+  and at k = 4 on C2 (the logN 15 chain of fifteen 58-bit primes)
   (software/kklss/mkbfv/evaluator.go:85-152).
 
 The oracle runs in spawned worker processes (one case each) while the test
@@ -34,7 +34,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def oracle_results():
     """Every case's oracle output, computed in parallel in spawned workers."""
-    workers = max(1, min(len(BC.CASES), (os.cpu_count() or 2) - 1, 8))
+    workers = max(1, min(len(BC.CASES), (os.cpu_count() or 2) - 1, 9))
     ex = cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"))
     futs = {name: ex.submit(BC.oracle_output, name) for name in BC.CASES}
     yield futs
@@ -94,7 +94,8 @@ def test_kklss_ckks_serving_rings_bitexact(name, oracle_results):
     assert kg.precision_bits(H.kklss_ckks_decode(case, got, lv, sc), case.want) > 15
 
 
-@pytest.mark.parametrize("name", ["kklss_bfv_s14_k8", "kklss_bfv_c2_k4", "kklss_bfv_s16_k8"])
+@pytest.mark.parametrize("name", ["kklss_bfv_s14_k8", "kklss_bfv_c2_k4", "kklss_bfv_s15_k8",
+                                  "kklss_bfv_s16_k8"])
 def test_kklss_bfv_serving_rings_bitexact(name, oracle_results):
     case = BC.build(name)
     lit, k = case.lit, case.k
