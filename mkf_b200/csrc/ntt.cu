@@ -489,33 +489,29 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         uint64_t v[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[r] = data[MKF_DIDX(rowoff + r * T + t, N, kDbgNtt | 5)];
-        // the last pass stays in registers: lane t then holds points
-        // 8t..8t+7 of its row and stores them as four 16-byte words (every
-        // lane loaded its words before the first exchange, so the row can be
-        // overwritten in place)
-        ulonglong2 *out2 = reinterpret_cast<ulonglong2 *>(data + rowoff + 8 * t);
+        // the last pass leaves the row in the warp's tile region; it is
+        // stored from there in point order (lane t: points k*T + t), which
+        // writes whole sectors per instruction
         if (fp) {
             double vf[8];
 #pragma unroll
             for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
             const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
-            fwd_passes_f<LOGS, 32, 8, true, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
+            fwd_passes_f<LOGS, 32, 8, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                out2[j] = make_ulonglong2(canon_f(vf[2 * j], md.qd), canon_f(vf[2 * j + 1], md.qd));
+            for (int k = 0; k < 8; ++k)
+                data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[(sb0 ^ swz(k * T))]), md.qd);
         } else {
             const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
             if (lazy) {
-                fwd_passes<LOGS, true, true, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    out2[j] = make_ulonglong2(reduce_any(v[2 * j], q, md.one_sh),
-                                              reduce_any(v[2 * j + 1], q, md.one_sh));
+                for (int k = 0; k < 8; ++k)
+                    data[rowoff + k * T + t] = reduce_any(s[(sb0 ^ swz(k * T))], q, md.one_sh);
             } else {
-                fwd_passes<LOGS, false, true, false, true>(s, tw, q, c, t, v);
+                fwd_passes<LOGS, false, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    out2[j] = make_ulonglong2(reduce4(v[2 * j], q), reduce4(v[2 * j + 1], q));
+                for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = reduce4(s[(sb0 ^ swz(k * T))], q);
             }
         }
         return;
