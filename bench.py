@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--lanes", default="4,8,16", help="lane counts the batch autotuner tries")
     ap.add_argument("--plan-lanes", default="1,2",
                     help="lane counts tried for the headline key-fused plan")
+    ap.add_argument("--plan-forms", default="graph,persistent",
+                    help="batch plan forms tried: graph (the lanes' kernels in a CUDA graph), "
+                         "persistent (one launch of the persistent executor)")
     ap.add_argument("--tuning", default="",
                     help='launch choices as JSON, e.g. {"fuse_ip": 1, "ip_block": 256, '
                          '"modup_chunk": 24}, instead of autotuning (profiling runs)')
@@ -345,13 +348,19 @@ def random_limbs(g, moduli, n, count=1):
     return out
 
 
-def best_plan(ev, P, jobs, lanes_arg, cs, stream, reps=3):
-    """The key-fused batch plan (graph-captured) with the fastest lane count
-    of `lanes_arg`; returns (plan, lanes, {lanes: ms per launch})."""
+def best_plan(ev, P, jobs, lanes_arg, cs, stream, reps=3, forms="graph"):
+    """The key-fused batch plan (replayed from a CUDA graph) with the fastest
+    lane count of `lanes_arg` and form of `forms` ("graph": the lanes' kernels
+    in the graph; "persistent": the plan as one launch of the persistent
+    executor); returns (plan, label, {label: ms per launch})."""
     tried, best = {}, None
-    for lanes in [int(x) for x in lanes_arg.split(",") if x]:
-        b = ev.Batch(P, jobs, lanes=lanes, graph=True, fuse_keys=True)
+    cands = [(int(x), f) for f in forms.split(",") if f for x in lanes_arg.split(",") if x]
+    for lanes, form in cands:
+        label = f"{lanes}{' persistent' if form == 'persistent' else ''}"
+        b = ev.Batch(P, jobs, lanes=lanes, graph=True, fuse_keys=True,
+                     persistent=form == "persistent")
         b.launch(cs)
+        b.check()
         e0, e1 = __import__("torch").cuda.Event(enable_timing=True), \
             __import__("torch").cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -360,11 +369,12 @@ def best_plan(ev, P, jobs, lanes_arg, cs, stream, reps=3):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / reps
-        tried[lanes] = ms
+        b.check()
+        tried[label] = ms
         if best is None or ms < best[1]:
             if best is not None:
                 best[0].close()
-            best = (b, ms, lanes)
+            best = (b, ms, label)
         else:
             b.close()
     return best[0], best[2], tried
@@ -519,7 +529,8 @@ def run_c3(a, reps, ws, rank, local):
     pouts = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.batch)]
     pjobs = [("mkf", E, ins[j % nin][0], ins[j % nin][1], pouts[j], True, True)
              for j in range(a.batch)]
-    plan, plan_lanes, plan_tried = best_plan(ev, P, pjobs, a.plan_lanes, cs0, s0)
+    plan, plan_lanes, plan_tried = best_plan(ev, P, pjobs, a.plan_lanes, cs0, s0,
+                                             forms=a.plan_forms)
     for _ in range(a.warmup):
         plan.launch(cs0)
     torch.cuda.synchronize()
@@ -538,8 +549,10 @@ def run_c3(a, reps, ws, rank, local):
     launches = int(L.mkf_launch_count(0))
     total_ms = max_over_ranks(t0.elapsed_time(t1))
     value = ws * a.steps * a.batch / (total_ms / 1e3)
-    plan_res = {"lanes": plan_lanes, "kernels_per_step": plan.kernels, "graph": True,
-                "fuse_keys": True, "lanes_ms_per_step": plan_tried}
+    plan.check()
+    plan_res = {"lanes": int(plan_lanes.split()[0]), "kernels_per_step": plan.kernels, "graph": True,
+                "fuse_keys": True, "persistent": plan_lanes.endswith("persistent"),
+                "lanes_ms_per_step": plan_tried}
     plan.close()
     del pouts, pjobs
 
@@ -673,7 +686,7 @@ def run_c3(a, reps, ws, rank, local):
         pouts8 = [ev.Ciphertext(P, k + 1, lo8, True) for _ in range(a.batch)]
         pjobs8 = [("mkf", E, ins8[j % nin][0], ins8[j % nin][1], pouts8[j], True, True)
                   for j in range(a.batch)]
-        plan8, lanes8, _ = best_plan(ev, P, pjobs8, a.plan_lanes, cs0, s0)
+        plan8, lanes8, tried8 = best_plan(ev, P, pjobs8, a.plan_lanes, cs0, s0, forms=a.plan_forms)
         for _ in range(a.warmup):
             plan8.launch(cs0)
         torch.cuda.synchronize()
@@ -689,7 +702,8 @@ def run_c3(a, reps, ws, rank, local):
         del pouts8, pjobs8
         lat8.sort()
         lvl8 = {"level": l8, "plain": ws * plain_steps / (max_over_ranks(sum(lat8)) / 1e3),
-                "batched": ws * a.steps * a.batch / (pms8 / 1e3), "plan_lanes": lanes8,
+                "batched": ws * a.steps * a.batch / (pms8 / 1e3), "plan": lanes8,
+                "plan_ms_per_step": tried8,
                 "streams": ws * a.steps * a.batch / (ms8 / 1e3), "unit": "mult+relin ops/s",
                 "latency_ms": {"p50": lat8[len(lat8) // 2],
                                "p99": lat8[min(len(lat8) - 1, int(0.99 * len(lat8)))]}}
@@ -841,18 +855,22 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
     # autotune the lane count: time each candidate plan, keep the fastest
     tried = {}
     best = None
+    forms = [f for f in a.plan_forms.split(",") if f]
     for lanes in [int(x) for x in a.lanes.split(",") if x]:
         for fuse in (False, True):
-            b = ev.Batch(P0, items, lanes=lanes, graph=True, fuse_keys=fuse)
-            ms = timed(lambda: b.launch(cs), reps)
-            tried[f"{lanes}{' fused' if fuse else ''}"] = ms
-            if best is None or ms < best[1]:
-                if best is not None:
-                    best[0].close()
-                best = (b, ms, lanes, fuse)
-            else:
-                b.close()
-    b, batch_ms, lanes, fuse = best
+            for form in forms:
+                pers = form == "persistent"
+                b = ev.Batch(P0, items, lanes=lanes, graph=True, fuse_keys=fuse, persistent=pers)
+                ms = timed(lambda: b.launch(cs), reps)
+                b.check()
+                tried[f"{lanes}{' fused' if fuse else ''}{' persistent' if pers else ''}"] = ms
+                if best is None or ms < best[1]:
+                    if best is not None:
+                        best[0].close()
+                    best = (b, ms, lanes, fuse, pers)
+                else:
+                    b.close()
+    b, batch_ms, lanes, fuse, pers = best
     L.mkf_launch_count(1)
     batch_ms = timed(lambda: b.launch(cs), reps)
     kernels = int(L.mkf_launch_count(0)) // (reps + max(1, a.warmup))
@@ -870,7 +888,7 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
                     it[1].MulRelin(it[2], it[3], it[4], rescale=True, materialize=True, stream=cs)
 
             p_ms = timed(plain_sub, reps)
-            bb = ev.Batch(P0, sub, lanes=lanes, graph=True, fuse_keys=fuse)
+            bb = ev.Batch(P0, sub, lanes=lanes, graph=True, fuse_keys=fuse, persistent=pers)
             b_ms = timed(lambda: bb.launch(cs), reps)
             bb.close()
             buckets[f"{name}_k{kb}"] = {"products": len(sub), "plain_ms": p_ms, "batched_ms": b_ms,
@@ -881,7 +899,7 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
            "products": n,
            "plain": {"value": n / (plain_ms / 1e3), "unit": "mult+relin ops/s", "ms": plain_ms},
            "batched": {"value": n / (batch_ms / 1e3), "unit": "mult+relin ops/s", "ms": batch_ms,
-                       "lanes": lanes, "graph": True, "fuse_keys": fuse,
+                       "lanes": lanes, "graph": True, "fuse_keys": fuse, "persistent": pers,
                        "kernels_per_launch": kernels},
            "batched_over_plain": plain_ms / batch_ms,
            "autotune_plan_ms": tried,

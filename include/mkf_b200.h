@@ -301,6 +301,23 @@ typedef struct mkf_batch mkf_batch;
  * ceil(jobs of the bundle / lanes), capped at 16 and by the scratch the
  * lanes may take (32 GiB in all); outputs stay bit-identical. */
 #define MKF_BATCH_FUSE_KEYS 2
+/* Run the whole plan as ONE launch of a persistent executor: the plan
+ * records every lane's kernel launches (grid and arguments) instead of
+ * issuing them, and one CTA per resident slot (two 512-thread CTAs per SM)
+ * takes (launch, block range) items from a queue in device memory, waits
+ * until the launch before its own in the same lane has finished, and runs
+ * the recorded kernel's body on its blocks (256-thread bodies two to a
+ * CTA).  Every wait is bounded (2 s); a wait that runs out marks the plan
+ * failed (mkf_batch_check) and the launch still ends.  Available for
+ * MKF-CKKS jobs on rings of logN 13-16; a plan whose jobs launch anything
+ * the executor cannot run is refused (MKF_ERR_INVALID_ARG).  Combines with
+ * MKF_BATCH_GRAPH (the queue reset and the launch replayed from a graph)
+ * and MKF_BATCH_FUSE_KEYS; outputs stay bit-identical. */
+#define MKF_BATCH_PERSISTENT 4
+/* Test hook of the persistent form: the last recorded launch waits for one
+ * item more than its predecessor has, so its wait (bounded at 20 ms) runs
+ * out and mkf_batch_check reports MKF_ERR_TIMEOUT. */
+#define MKF_BATCH_TEST_STALL 256
 /* Validates every job (job.status; the first failure is returned and no
  * plan is made), spreads the jobs over `lanes` concurrent streams of their
  * context (longest job first onto the least-loaded lane), sizes each lane's
@@ -315,8 +332,12 @@ mkf_status mkf_batch_create(mkf_ctx *ctx, mkf_job *jobs, int n, int lanes, int f
  * (operand contents may change between launches; handles may not). */
 mkf_status mkf_batch_launch(mkf_batch *batch, void *stream);
 void mkf_batch_destroy(mkf_batch *batch);
-/* Kernels one launch of the plan issues. */
+/* Kernels one launch of the plan issues (1 for a persistent plan). */
 uint64_t mkf_batch_kernels(const mkf_batch *batch);
+/* Waits for the plan's last launch and reports its outcome: MKF_OK, a CUDA
+ * error, or MKF_ERR_TIMEOUT when a persistent plan's bounded wait ran out
+ * (its outputs are then not valid). */
+mkf_status mkf_batch_check(mkf_batch *batch);
 /* One-shot: create (no graph, min(n, 8) lanes), launch on `stream`, destroy. */
 mkf_status mkf_mulrelin_batch(mkf_ctx *ctx, mkf_job *jobs, int n, void *stream);
 

@@ -60,6 +60,8 @@ SLOT_MUL_ADD, SLOT_ADD_C0, SLOT_MUL = 0, 1, 2
 JOB_MKF, JOB_KKLSS = 1, 2
 BATCH_GRAPH = 1
 BATCH_FUSE_KEYS = 2
+BATCH_PERSISTENT = 4
+BATCH_TEST_STALL = 256
 
 
 class Job(ctypes.Structure):
@@ -150,6 +152,7 @@ def lib():
         "mkf_batch_launch": (i, [vp, vp]),
         "mkf_batch_destroy": (None, [vp]),
         "mkf_batch_kernels": (ctypes.c_uint64, [vp]),
+        "mkf_batch_check": (i, [vp]),
         "mkf_mulrelin_batch": (i, [vp, ctypes.POINTER(Job), i, vp]),
         "mkf_mkf_fold": (i, [vp, vp, vp, vp, vp]),
         "mkf_mkf_materialize": (i, [vp, vp, vp, vp]),

@@ -284,12 +284,11 @@ mkf_status prepare_kklss(mkf_ctx *ctx, const mkf_ct *op0, const mkf_ct *op1,
             uint64_t *t = a.take((size_t)(k + 1) * w);
             o[j].data = t;
             if (a.dry) continue;
-            cudaMemsetAsync(t, 0, (size_t)(k + 1) * w * 8, st);
-            cudaMemcpyAsync(t, aa[j]->src, w * 8, cudaMemcpyDeviceToDevice, st);
+            fill_async(t, 0, (size_t)(k + 1) * w * 8, st);
+            copy_rows_async(t, w, aa[j]->src, w, w, 1, st);
             for (size_t i = 0; i < aa[j]->pos.size(); ++i)
-                cudaMemcpyAsync(t + (long long)(aa[j]->pos[i] + 1) * w,
-                                aa[j]->src + (long long)(i + 1) * aa[j]->src_cs, w * 8,
-                                cudaMemcpyDeviceToDevice, st);
+                copy_rows_async(t + (long long)(aa[j]->pos[i] + 1) * w, w,
+                                aa[j]->src + (long long)(i + 1) * aa[j]->src_cs, w, w, 1, st);
         }
         return kklss_mulrelin(ctx->c, a, st, bfv ? kBFV : kCKKS, k, level, o[0], o[1], kp, crs, nb, od, ocs);
     };

@@ -129,6 +129,83 @@ MKF_DEV void pdl_enter() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+
+// The block a kernel body runs as.  A stand-alone kernel passes its own CTA
+// (CtaBlk, whose indices are the special registers); the persistent executor
+// runs bodies as virtual blocks taken from a work queue (VBlk), two 256-thread
+// blocks side by side in one 512-thread CTA, each with its own named barrier
+// and shared memory.
+struct CtaBlk {
+    uint64_t *sm; // the block's shared memory
+    __device__ __forceinline__ unsigned bx() const { return blockIdx.x; }
+    __device__ __forceinline__ unsigned by() const { return blockIdx.y; }
+    __device__ __forceinline__ unsigned bz() const { return blockIdx.z; }
+    __device__ __forceinline__ unsigned nz() const { return gridDim.z; }
+    __device__ __forceinline__ unsigned t() const { return threadIdx.x; }
+    __device__ __forceinline__ unsigned nthreads() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct VBlk {
+    uint3 id, n;      // block index and grid size of the recorded launch
+    unsigned tt;      // thread index within the block
+    unsigned bar, nt; // barrier: 0 = the CTA's own, else named barrier `bar` of nt threads
+    uint64_t *sm;
+    __device__ __forceinline__ unsigned bx() const { return id.x; }
+    __device__ __forceinline__ unsigned by() const { return id.y; }
+    __device__ __forceinline__ unsigned bz() const { return id.z; }
+    __device__ __forceinline__ unsigned nz() const { return n.z; }
+    __device__ __forceinline__ unsigned t() const { return tt; }
+    __device__ __forceinline__ unsigned nthreads() const { return nt; }
+    __device__ __forceinline__ void sync() const {
+        if (bar == 0)
+            __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nt) : "memory");
+    }
+};
+// A load of data that an earlier stage wrote: through the read-only path in a
+// stand-alone kernel, a plain (coherent) load inside the persistent executor,
+// where the producer ran earlier in the same launch.
+template <bool PERS, typename T> MKF_DEV T ldp(const T *p) {
+    if constexpr (PERS)
+        return *p;
+    else
+        return __ldg(p);
+}
+
+// A kernel's arguments stored as one trivially copyable record, the same
+// layout on the host (where a launch is recorded) and on the device (where
+// the persistent executor reads it back).
+template <typename... T> struct ArgPack;
+template <> struct ArgPack<> {
+    __host__ __device__ ArgPack() {}
+};
+template <typename H, typename... T> struct ArgPack<H, T...> {
+    H h;
+    ArgPack<T...> t;
+    __host__ __device__ ArgPack(const H &h_, const T &...t_) : h(h_), t(t_...) {}
+};
+
+// Launch recording: while a recorder is installed on the calling host thread,
+// PdlLaunch and the copy/fill helpers hand their work to it instead of
+// issuing it on the stream (the persistent batch plans are built this way).
+struct LaunchRecorder {
+    virtual void kernel(const void *fn, dim3 grid, dim3 block, size_t smem, const void *args,
+                        size_t bytes) = 0;
+    virtual void copy_rows(uint64_t *dst, long long dst_stride, const uint64_t *src,
+                           long long src_stride, long long words, int rows) = 0;
+    virtual void fill(void *p, int value, size_t bytes) = 0;
+
+  protected:
+    ~LaunchRecorder() = default;
+};
+LaunchRecorder *&launch_recorder();
+// rows x words 64-bit words, device to device (cudaMemcpy2DAsync)
+void copy_rows_async(uint64_t *dst, long long dst_stride, const uint64_t *src, long long src_stride,
+                     long long words, int rows, cudaStream_t st);
+// cudaMemsetAsync
+void fill_async(void *p, int value, size_t bytes, cudaStream_t st);
+
 struct PdlLaunch {
     dim3 g, b;
     size_t smem;
@@ -137,6 +214,11 @@ struct PdlLaunch {
         : g(grid), b(block), smem(shared), st(stream) {}
     template <typename... KArgs, typename... Args>
     void operator()(void (*kernel)(KArgs...), Args... args) const {
+        if (LaunchRecorder *r = launch_recorder()) {
+            const ArgPack<KArgs...> pk(static_cast<KArgs>(args)...);
+            r->kernel(reinterpret_cast<const void *>(kernel), g, b, smem, &pk, sizeof pk);
+            return;
+        }
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;

@@ -66,9 +66,7 @@ ModMap qmmap(const Context &c) { return ModMap{0, 0, c.qmidx(0)}; }
 
 void d2d2(uint64_t *dst, long long dst_stride, const uint64_t *src, long long src_stride,
           long long words, int rows, cudaStream_t st) {
-    if (rows <= 0 || words <= 0) return;
-    cudaMemcpy2DAsync(dst, dst_stride * 8, src, src_stride * 8, words * 8, rows,
-                      cudaMemcpyDeviceToDevice, st);
+    copy_rows_async(dst, dst_stride, src, src_stride, words, rows, st);
 }
 
 // Prepares a ModDown of npolys QP accumulators (NTT domain, level L1):
@@ -102,7 +100,7 @@ CombineSpec pdown(const Context &c, const uint64_t *acc, long long acc_pstride, 
     return s;
 }
 
-void fill_ones(uint8_t *p, int n, cudaStream_t st) { cudaMemsetAsync(p, 1, n, st); }
+void fill_ones(uint8_t *p, int n, cudaStream_t st) { fill_async(p, 1, (size_t)n, st); }
 
 } // namespace
 
@@ -223,7 +221,7 @@ static void fold_sides(const Context &c, cudaStream_t st, bool bfv, int k, int l
     if (!bfv) ntt_forward(c, lsq(f.tmp, poly, L1), 2 * nops, st);
     for (int s = 0; s < nops; ++s) {
         d2d2(F + 2 * s * poly, poly, ops[s].data, ops[s].cs, poly, 1, st);
-        cudaMemsetAsync(F + (2 * s + 1) * poly, 0, poly * 8, st);
+        fill_async(F + (2 * s + 1) * poly, 0, (size_t)poly * 8, st);
     }
     CombineSpec cs = pdown(c, f.acc, qp, f.tmp, poly, F, poly, 1);
     cs.x_tstride = 2 * nops * qp;

@@ -17,9 +17,12 @@
 
 #include <mutex>
 #include <set>
+#include <type_traits>
 #include <utility>
 
+#include "kernels_dev.cuh"
 #include "modup.cuh"
+#include "persistent.h"
 
 namespace mkf {
 
@@ -265,7 +268,7 @@ MKF_DEV TwD ldtwd_s(const TwD *p) {
 // CONV: the words enter the float64 transform and are stored as the bits of
 // their centered doubles; 1: any word below 2^52, 2: canonical words.
 template <int LOGS, bool COLS, int CONV = 0>
-MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double qi = 0.0,
+MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, int bx, double qi = 0.0,
                        double qd = 0.0) {
     constexpr int S = 1 << LOGS, C = kTile / S;
     // columns: element e of this thread is point e*S/8 + tid/C of column
@@ -280,12 +283,12 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
         if (COLS) {
             const int r = idx / C, cc = idx % C;
             a = cbase ^ swz(e << (LOGS - 3));
-            MKF_DCHECK_LT(blockIdx.x * C + cc, R, kDbgNtt | 2);
-            v = data[blockIdx.x * C + r * R + cc];
+            MKF_DCHECK_LT(bx * C + cc, R, kDbgNtt | 2);
+            v = data[bx * C + r * R + cc];
         } else {
             const int cc = idx / S, j = idx % S;
             a = saddr<S>(cc, j);
-            v = data[(long long)blockIdx.x * kTile + idx];
+            v = data[(long long)bx * kTile + idx];
         }
         if (CONV == 1) v = (uint64_t)__double_as_longlong(reduce_f(u64_to_f(v), qi, qd));
         if (CONV == 2) v = (uint64_t)__double_as_longlong(centered_f(v, (uint64_t)qd));
@@ -298,8 +301,8 @@ MKF_DEV void tile_load(uint64_t *s, const uint64_t *data, int R, int tid, double
 enum StoreRed { kRedNone, kRed4, kRedAny, kRed2q, kRedF };
 
 template <int LOGS, bool COLS>
-MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const DevModulus &md,
-                        StoreRed red) {
+MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, int bx,
+                        const DevModulus &md, StoreRed red) {
     constexpr int S = 1 << LOGS, C = kTile / S;
     const int cbase = saddr<S>(tid % C, tid / C); // as in tile_load
 #pragma unroll
@@ -310,11 +313,11 @@ MKF_DEV void tile_store(const uint64_t *s, uint64_t *data, int R, int tid, const
         if (COLS) {
             const int r = idx / C, cc = idx % C;
             v = s[cbase ^ swz(e << (LOGS - 3))];
-            o = blockIdx.x * C + r * R + cc;
+            o = bx * C + r * R + cc;
         } else {
             const int cc = idx / S, j = idx % S;
             v = s[saddr<S>(cc, j)];
-            o = (long long)blockIdx.x * kTile + idx;
+            o = (long long)bx * kTile + idx;
         }
         if (red == kRed4) v = reduce4(v, md.q);
         else if (red == kRedAny) v = reduce_any(v, md.q, md.one_sh);
@@ -458,13 +461,12 @@ MKF_DEV void fwd_passes_f(uint64_t *s, const TwD *tw, double q, double qi, int c
     }
 }
 
-template <int LOGS, bool COLS>
-__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
-    pdl_enter();
+// s: the 4096-word tile; twdyn: the column pass's staged twiddles (S entries).
+template <int LOGS, bool COLS, class B>
+MKF_DEV void ntt_fwd_phase_body(const B &bk, const NttArgs &a, uint64_t *s, uint64_t *twdyn) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    __shared__ uint64_t s[kTile];
     const int limbs = a.ls.limbs;
-    const int poly = blockIdx.y / limbs, l = blockIdx.y % limbs;
+    const int poly = bk.by() / limbs, l = bk.by() % limbs;
     const int m = a.ls.mod_of(l);
     const DevModulus md = a.mods[m];
     const uint64_t q = md.q;
@@ -472,10 +474,10 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
     const int N = 1 << a.logN;
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
-    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int tid = bk.t(), c = tid / T, t = tid % T;
     const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     if (!COLS && a.own_alpha) {
-        const int d = (blockIdx.y / limbs) % a.own_ndigits, start = d * a.own_alpha;
+        const int d = (bk.by() / limbs) % a.own_ndigits, start = d * a.own_alpha;
         if (l < a.ls.nq && l >= start && l < start + digit_ns(a.own_level, a.own_alpha, d)) return;
     }
     // float64 limbs: the column pass converts the input words, the row pass
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         // row phase: each row belongs to T lanes of one warp; its words are
         // loaded straight into the first radix-8 pass, and no block-wide
         // barrier is needed.
-        const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+        const long long rowoff = (long long)(bk.bx() * C + c) * S;
         uint64_t v[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[r] = data[MKF_DIDX(rowoff + r * T + t, N, kDbgNtt | 5)];
@@ -496,13 +498,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
             double vf[8];
 #pragma unroll
             for (int r = 0; r < 8; ++r) vf[r] = __longlong_as_double((long long)v[r]);
-            const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            const TwD *twd = a.tw2d + (size_t)m * N + (size_t)(bk.bx() * C + c) * S;
             fwd_passes_f<LOGS, 32, 8, false, false, true>(s, twd, md.qd, md.qinvd, c, t, vf);
 #pragma unroll
             for (int k = 0; k < 8; ++k)
                 data[rowoff + k * T + t] = canon_f(__longlong_as_double((long long)s[(sb0 ^ swz(k * T))]), md.qd);
         } else {
-            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(bk.bx() * C + c) * S;
             if (lazy) {
                 fwd_passes<LOGS, true, false, false, true>(s, tw, q, c, t, v);
 #pragma unroll
@@ -517,12 +519,11 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         return;
     }
     if (fp)
-        tile_load<LOGS, true, 1>(s, data, R, tid, md.qinvd, md.qd);
+        tile_load<LOGS, true, 1>(s, data, R, tid, bk.bx(), md.qinvd, md.qd);
     else
-        tile_load<LOGS, true>(s, data, R, tid);
+        tile_load<LOGS, true>(s, data, R, tid, bk.bx());
     // the column pass stages its table (S entries, shared by every column) in
     // shared memory
-    extern __shared__ __align__(16) uint64_t twdyn[];
     Tw *tws = reinterpret_cast<Tw *>(twdyn);
     {
         const ulonglong2 *twg =
@@ -531,15 +532,23 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
         ulonglong2 *d = reinterpret_cast<ulonglong2 *>(tws);
         for (int i = tid; i < S; i += kPhaseThreads) d[i] = __ldg(twg + i);
     }
-    __syncthreads();
+    bk.sync();
     if (fp)
         fwd_passes_f<LOGS, 8, 32, false, true>(s, reinterpret_cast<const TwD *>(tws), md.qd, md.qinvd, c, t);
     else if (lazy)
         fwd_passes<LOGS, true, false, true>(s, tws, q, c, t);
     else
         fwd_passes<LOGS, false, false, true>(s, tws, q, c, t);
-    __syncthreads();
-    tile_store<LOGS, true>(s, data, R, tid, md, kRedNone);
+    bk.sync();
+    tile_store<LOGS, true>(s, data, R, tid, bk.bx(), md, kRedNone);
+}
+
+template <int LOGS, bool COLS>
+__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_fwd_phase(NttArgs a) {
+    pdl_enter();
+    __shared__ uint64_t s[kTile];
+    extern __shared__ __align__(16) uint64_t twdyn[];
+    ntt_fwd_phase_body<LOGS, COLS>(CtaBlk{s}, a, s, twdyn);
 }
 
 // Dynamic shared memory of ntt_fwd_phase: its staged twiddles.
@@ -592,22 +601,23 @@ constexpr int kColThreads = 256, kColWords = 2048;
 // staged source limb
 constexpr size_t kColSmem = (size_t)kColWords * 8 * 3;
 
-template <int LOGS>
-__global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
-    pdl_enter();
+// PERS: the persistent executor's form, whose y_i and corrections were
+// written earlier in the same launch (coherent loads, not the read-only path).
+template <int LOGS, bool PERS, class B>
+MKF_DEV void ntt_fwd_digits_col_body(const B &bk, const NttArgs &a, const DigitSrc &src) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kColWords / S, NW = kColWords;
-    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t *dsm = bk.sm;
     uint64_t *ys = dsm + 2 * NW;       // [C][S] the staged one-limb source
     const int limbs = a.ls.limbs;
-    const int pd = blockIdx.y, poly = pd / src.ndigits, d = pd % src.ndigits;
+    const int pd = bk.by(), poly = pd / src.ndigits, d = pd % src.ndigits;
     const int N = 1 << a.logN, R = 1 << a.n2;
     const int L1 = src.level + 1;
     const int start = d * src.alpha;
     const int ns = digit_ns(src.level, src.alpha, d);
     const bool msum = ns >= 2 && src.tabs;
-    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int tid = bk.t(), c = tid / T, t = tid % T;
     const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
-    const int col0 = blockIdx.x * C;
+    const int col0 = bk.bx() * C;
     // a one-limb digit's source limb is staged for the block's columns; the
     // y_i of a multSum digit are read from L2 for every limb
     if (!msum && ns == 1) {
@@ -617,7 +627,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             ys[MKF_DIDX(cc * S + r, NW, kDbgNtt | 6)] = xs[(long long)r * R + col0 + cc];
         }
     }
-    __syncthreads();
+    bk.sync();
     const ModUpTab *tb = msum ? src.tabs + d * (src.alpha + 1) + ns : nullptr;
     // the float64 corrections of this thread's 8 first-pass words are the
     // same for every target limb: loaded once, one byte each
@@ -625,14 +635,14 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
     if (msum) {
         const uint8_t *vl = src.v + (long long)pd * N + (long long)(col0 + c) * S + t;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) vpk[r >> 2] |= (uint32_t)__ldg(vl + r * T) << (8 * (r & 3));
+        for (int r = 0; r < 8; ++r) vpk[r >> 2] |= (uint32_t)ldp<PERS>(vl + r * T) << (8 * (r & 3));
     }
     // this block's share of the limbs (grid.z splits them, against the tail
     // of the last wave)
-    const int per = (limbs + gridDim.z - 1) / gridDim.z;
-    const int l_end = min(limbs, (int)(blockIdx.z + 1) * per);
+    const int per = (limbs + bk.nz() - 1) / bk.nz();
+    const int l_end = min(limbs, (int)(bk.bz() + 1) * per);
     int buf = 0;
-    for (int l = blockIdx.z * per; l < l_end; ++l) {
+    for (int l = bk.bz() * per; l < l_end; ++l) {
         const bool own_limb = l < L1 && l >= start && l < start + ns;
         uint64_t *dst = a.ls.base + (long long)pd * a.ls.poly_stride + (long long)l * N + col0;
         if (own_limb && src.own.p[0]) {
@@ -668,7 +678,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
                 const int r = idx / C, cc = idx % C;
                 s[saddr<S>(cc, r)] = mred(xs[(long long)r * R + col0 + cc], md.mont1, q, md.qinv);
             }
-            __syncthreads();
+            bk.sync();
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
                 const uint64_t x = s[saddr<S>(c, elem<LOGS>(0, t, r))];
@@ -701,7 +711,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 #pragma unroll
                     for (int r = 0; r < 8; ++r)
                         acc[r] = __dadd_rn(acc[r], mulmod_f(__longlong_as_double(
-                                                                    (long long)__ldg(yl + (long long)i * N + r * T)),
+                                                                    (long long)ldp<PERS>(yl + (long long)i * N + r * T)),
                                                                 cw, cq, md.qd));
                 }
 #pragma unroll
@@ -727,7 +737,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
 #pragma unroll
                         for (int r = 0; r < 4; ++r) {
                             const uint64_t yv = (uint64_t)__double_as_longlong(__dadd_rn(
-                                                    __longlong_as_double((long long)__ldg(yl + (long long)i * N + (h + r) * T)),
+                                                    __longlong_as_double((long long)ldp<PERS>(yl + (long long)i * N + (h + r) * T)),
                                                     yoff)) - ysub;
                             mac128(lo[r], hi[r], yv, b);
                         }
@@ -754,7 +764,7 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             fwd_passes<LOGS, false, false, false, true>(s, a.tw1 + (size_t)m * S, q, c, t, vi);
         }
         // the tile holds every column of the block: store it row-major
-        __syncthreads();
+        bk.sync();
         {
             // element e of this thread is point e*RS + tid/C of column tid%C:
             // its tile address is the thread's base XOR a constant and its
@@ -771,6 +781,13 @@ __global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, 
             for (int e = 0; e < 8; ++e) db[(long long)e * RS * R] = s[tb ^ swz(e * RS)];
         }
     }
+}
+
+template <int LOGS>
+__global__ void __launch_bounds__(kColThreads, 4) ntt_fwd_digits_col(NttArgs a, DigitSrc src) {
+    pdl_enter();
+    extern __shared__ __align__(16) uint64_t dsm[];
+    ntt_fwd_digits_col_body<LOGS, false>(CtaBlk{dsm}, a, src);
 }
 
 // The butterfly passes of an inverse phase.  COLS: the second (last) inverse
@@ -884,26 +901,25 @@ MKF_DEV void inv_passes_f(uint64_t *s, const TwD *tw, const DevModulus &md, int 
     }
 }
 
-template <int LOGS, bool COLS>
-__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
-    pdl_enter();
+// s: the 4096-word tile.
+template <int LOGS, bool COLS, class B>
+MKF_DEV void ntt_inv_phase_body(const B &bk, const NttArgs &a, uint64_t *s) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    __shared__ uint64_t s[kTile];
     const int limbs = a.ls.limbs;
-    const int poly = blockIdx.y / limbs, l = blockIdx.y % limbs;
+    const int poly = bk.by() / limbs, l = bk.by() % limbs;
     const int m = a.ls.mod_of(l);
     const DevModulus md = a.mods[m];
     const bool lazy = md.q < kLazyBound;
     const int N = 1 << a.logN;
     const int R = 1 << a.n2;
     uint64_t *data = a.ls.base + (long long)poly * a.ls.poly_stride + (long long)l * N;
-    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int tid = bk.t(), c = tid / T, t = tid % T;
     const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     if (!COLS) {
         // row phase: each row belongs to T lanes of one warp, loaded into and
         // stored from the warp's tile region in point order (lane t: points
         // k*T + t); no block-wide barrier
-        const long long rowoff = (long long)(blockIdx.x * C + c) * S;
+        const long long rowoff = (long long)(bk.bx() * C + c) * S;
         const bool fp = md.q < kFp64Bound;
         const uint64_t *rd = a.src_poly0 >= 0 ? a.src.poly(a.src_poly0 + poly) + (long long)l * N : data;
         // the first inverse pass holds points 8t..8t+7: lane t loads them as
@@ -921,12 +937,12 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) wf[r] = centered_f(w[r], md.q);
             // the last pass holds points k*T + t (point order): stored directly
-            inv_passes_f<LOGS, false, true, true>(s, a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S, md, c,
+            inv_passes_f<LOGS, false, true, true>(s, a.tw2d + (size_t)m * N + (size_t)(bk.bx() * C + c) * S, md, c,
                                                   t, wf, wf);
 #pragma unroll
             for (int k = 0; k < 8; ++k) data[rowoff + k * T + t] = (uint64_t)__double_as_longlong(wf[k]);
         } else {
-            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+            const Tw *tw = a.tw2 + (size_t)m * N + (size_t)(bk.bx() * C + c) * S;
             if (lazy) {
                 inv_passes<LOGS, false, true, true, true>(s, tw, md, c, t, w, w);
                 // the first phase hands the second one values below 2q
@@ -944,28 +960,35 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
         // float64 limbs: the row phase converts the canonical input, the
         // column phase reads its doubles and stores canonical words
         if (COLS)
-            tile_load<LOGS, true>(s, data, R, tid);
+            tile_load<LOGS, true>(s, data, R, tid, bk.bx());
         else
-            tile_load<LOGS, false, 2>(s, data, R, tid, md.qinvd, md.qd);
-        __syncthreads();
+            tile_load<LOGS, false, 2>(s, data, R, tid, bk.bx(), md.qinvd, md.qd);
+        bk.sync();
         const TwD *tw = COLS ? a.tw1d + (size_t)m * (1 << a.n1)
-                             : a.tw2d + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+                             : a.tw2d + (size_t)m * N + (size_t)(bk.bx() * C + c) * S;
         inv_passes_f<LOGS, COLS>(s, tw, md, c, t);
-        __syncthreads();
-        tile_store<LOGS, COLS>(s, data, R, tid, md, COLS ? kRedF : kRedNone);
+        bk.sync();
+        tile_store<LOGS, COLS>(s, data, R, tid, bk.bx(), md, COLS ? kRedF : kRedNone);
         return;
     }
-    tile_load<LOGS, COLS>(s, data, R, tid);
-    __syncthreads();
+    tile_load<LOGS, COLS>(s, data, R, tid, bk.bx());
+    bk.sync();
     const Tw *tw = COLS ? a.tw1 + (size_t)m * (1 << a.n1)
-                        : a.tw2 + (size_t)m * N + (size_t)(blockIdx.x * C + c) * S;
+                        : a.tw2 + (size_t)m * N + (size_t)(bk.bx() * C + c) * S;
     if (lazy)
         inv_passes<LOGS, COLS, true>(s, tw, md, c, t);
     else
         inv_passes<LOGS, COLS, false>(s, tw, md, c, t);
-    __syncthreads();
+    bk.sync();
     // the first phase hands the second one values below 2q
-    tile_store<LOGS, COLS>(s, data, R, tid, md, (!COLS && lazy) ? kRed2q : kRedNone);
+    tile_store<LOGS, COLS>(s, data, R, tid, bk.bx(), md, (!COLS && lazy) ? kRed2q : kRedNone);
+}
+
+template <int LOGS, bool COLS>
+__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_inv_phase(NttArgs a) {
+    pdl_enter();
+    __shared__ uint64_t s[kTile];
+    ntt_inv_phase_body<LOGS, COLS>(CtaBlk{s}, a, s);
 }
 
 template <int LOG1, int LOG2>
@@ -1048,17 +1071,16 @@ constexpr size_t kRowIpSmem = 3 * kTile * sizeof(uint64_t);
 // NTT-domain input instead.  MRed(v, key) = v*key*2^-64 mod q is canonical
 // for any 64-bit v, so the lazy integer outputs need no reduction, and the
 // sum equals the stand-alone inner product's exactly.
-template <int LOGS>
-__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a, DigitIpArgs g) {
-    pdl_enter();
+template <int LOGS, class B>
+MKF_DEV void ntt_digits_row_ip_body(const B &bk, const NttArgs &a, const DigitIpArgs &g) {
     constexpr int S = 1 << LOGS, T = S / 8, C = kTile / S;
-    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t *dsm = bk.sm;
     uint64_t *s = dsm;
-    // the inputs of one key group are adjacent blocks (blockIdx.x = row tile *
+    // the inputs of one key group are adjacent blocks (bk.bx() = row tile *
     // nin + input), so the key rows one of them reads from HBM are still in
     // L2 when the others read them: each key word crosses HBM about once
-    const int l = blockIdx.y;
-    const int grp = blockIdx.z, sidx = blockIdx.x % g.nin, tile = blockIdx.x / g.nin;
+    const int l = bk.by();
+    const int grp = bk.bz(), sidx = bk.bx() % g.nin, tile = bk.bx() / g.nin;
     const int poly = sidx * g.groups + grp;
     const int m = a.ls.mod_of(l);
     const DevModulus md = a.mods[m];
@@ -1066,7 +1088,7 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
     const bool lazy = q < kLazyBound;
     const bool fp = q < kFp64Bound;
     const int N = 1 << a.logN;
-    const int tid = threadIdx.x, c = tid / T, t = tid % T;
+    const int tid = bk.t(), c = tid / T, t = tid % T;
     const int sb0 = saddr<S>(c, t); // point order: point k*T + t at sb0 ^ swz(k * T)
     const long long rowoff = (long long)(tile * C + c) * S;
     // accumulators of this row, point order (lane t: points k*T + t)
@@ -1169,6 +1191,13 @@ __global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a,
         o0[k * T] = acc0[k * T];
         o1[k * T] = acc1[k * T];
     }
+}
+
+template <int LOGS>
+__global__ void __launch_bounds__(kPhaseThreads, 2) ntt_digits_row_ip(NttArgs a, DigitIpArgs g) {
+    pdl_enter();
+    extern __shared__ __align__(16) uint64_t dsm[];
+    ntt_digits_row_ip_body<LOGS>(CtaBlk{dsm}, a, g);
 }
 
 void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig, int npolys,
@@ -1338,6 +1367,265 @@ void ntt_inverse_from(const Context &c, const OwnNtt &src, const LimbSet &ls, in
                       cudaStream_t st) {
     launch_split(c, ls, npolys, st, true, &src);
 }
+
+// ---------------------------------------------------------------------------
+// Persistent executor (persistent.h).  The CTAs of one launch take items
+// (recorded launch, virtual block range) from a queue in the order the plan
+// laid them out, wait until the launch before theirs in the same lane has
+// finished all its items, run the launch's kernel body on their virtual
+// blocks, and count the item as finished.  Every item's dependency comes
+// earlier in the queue, so it is held by a running CTA or done: the earliest
+// unfinished item can always run, and the launch ends.  A wait that exceeds
+// its bound (or finds another one expired) raises the error flag and goes
+// on, so the launch ends in every case; the host then reports the plan as
+// failed.
+// ---------------------------------------------------------------------------
+
+// Recorded copies and fills run as 256-thread bodies: block (x, y) moves
+// words [1024x, 1024x + 1024) of row y (bytes, for a fill not made of
+// whole aligned words).
+MKF_DEV void copy_rows_body(const VBlk &bk, const CopyRowsArgs &a) {
+    const long long base = (long long)bk.bx() * 1024 + bk.t();
+    const uint64_t *s = a.src + (long long)bk.by() * a.src_stride;
+    uint64_t *d = a.dst + (long long)bk.by() * a.dst_stride;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const long long i = base + k * 256;
+        if (i < a.words) d[i] = s[i];
+    }
+}
+MKF_DEV void fill_body(const VBlk &bk, const FillArgs &a) {
+    const unsigned long long base = (unsigned long long)bk.bx() * 1024 + bk.t();
+    if (((uintptr_t)a.p & 7) == 0 && (a.bytes & 7) == 0) {
+        const uint64_t v = 0x0101010101010101ull * (uint64_t)(a.value & 0xff);
+        uint64_t *w = reinterpret_cast<uint64_t *>(a.p);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const unsigned long long i = base + k * 256;
+            if (i < a.bytes / 8) w[i] = v;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const unsigned long long i = base + k * 256;
+            if (i < a.bytes) a.p[i] = (unsigned char)a.value;
+        }
+    }
+}
+
+// Reads a recorded argument record back as the kernel's parameter types and
+// calls f with them.
+template <class F> struct KernelPack;
+template <class... A> struct KernelPack<void(A...)> {
+    using type = ArgPack<A...>;
+    static constexpr int n = sizeof...(A);
+};
+template <int I> struct PackAt {
+    template <class P> MKF_DEV static const auto &get(const P &p) { return PackAt<I - 1>::get(p.t); }
+};
+template <> struct PackAt<0> {
+    template <class P> MKF_DEV static const auto &get(const P &p) { return p.h; }
+};
+template <class... A, class F, int... I>
+MKF_DEV void apply_pack(const ArgPack<A...> &p, F &f, std::integer_sequence<int, I...>) {
+    f(PackAt<I>::get(p)...);
+}
+template <class K, class F> MKF_DEV void run_pack(const unsigned char *args, F f) {
+    using KP = KernelPack<K>;
+    apply_pack(*reinterpret_cast<const typename KP::type *>(args), f,
+               std::make_integer_sequence<int, KP::n>{});
+}
+
+// One function per body kind, called with the item's virtual block and its
+// argument record (global memory, read-only for the whole launch).
+#define MKF_PERS_FN(KIND, SIG, ...)                                                                \
+    MKF_DEV void pers_##KIND(const VBlk &bk, const unsigned char *__restrict__ args) {             \
+        run_pack<SIG>(args, [&](const auto &...a) { __VA_ARGS__; });                               \
+    }
+MKF_PERS_FN(kBodyFwdCol6, void(NttArgs), ntt_fwd_phase_body<6, true>(bk, a..., bk.sm, bk.sm + kTile))
+MKF_PERS_FN(kBodyFwdCol7, void(NttArgs), ntt_fwd_phase_body<7, true>(bk, a..., bk.sm, bk.sm + kTile))
+MKF_PERS_FN(kBodyFwdCol8, void(NttArgs), ntt_fwd_phase_body<8, true>(bk, a..., bk.sm, bk.sm + kTile))
+MKF_PERS_FN(kBodyFwdRow7, void(NttArgs), ntt_fwd_phase_body<7, false>(bk, a..., bk.sm, bk.sm + kTile))
+MKF_PERS_FN(kBodyFwdRow8, void(NttArgs), ntt_fwd_phase_body<8, false>(bk, a..., bk.sm, bk.sm + kTile))
+MKF_PERS_FN(kBodyInvCol6, void(NttArgs), ntt_inv_phase_body<6, true>(bk, a..., bk.sm))
+MKF_PERS_FN(kBodyInvCol7, void(NttArgs), ntt_inv_phase_body<7, true>(bk, a..., bk.sm))
+MKF_PERS_FN(kBodyInvCol8, void(NttArgs), ntt_inv_phase_body<8, true>(bk, a..., bk.sm))
+MKF_PERS_FN(kBodyInvRow7, void(NttArgs), ntt_inv_phase_body<7, false>(bk, a..., bk.sm))
+MKF_PERS_FN(kBodyInvRow8, void(NttArgs), ntt_inv_phase_body<8, false>(bk, a..., bk.sm))
+MKF_PERS_FN(kBodyDigitsCol6, void(NttArgs, DigitSrc), ntt_fwd_digits_col_body<6, true>(bk, a...))
+MKF_PERS_FN(kBodyDigitsCol7, void(NttArgs, DigitSrc), ntt_fwd_digits_col_body<7, true>(bk, a...))
+MKF_PERS_FN(kBodyDigitsCol8, void(NttArgs, DigitSrc), ntt_fwd_digits_col_body<8, true>(bk, a...))
+MKF_PERS_FN(kBodyRowIp7, void(NttArgs, DigitIpArgs), ntt_digits_row_ip_body<7>(bk, a...))
+MKF_PERS_FN(kBodyRowIp8, void(NttArgs, DigitIpArgs), ntt_digits_row_ip_body<8>(bk, a...))
+MKF_PERS_FN(kBodyDigitsPrep, std::remove_reference_t<decltype(digits_prep_kernel)>, digits_prep_body(bk, a...))
+MKF_PERS_FN(kBodyModup4, void(ModUpArgs), modup_body<4>(bk, a...))
+MKF_PERS_FN(kBodyModup8, void(ModUpArgs), modup_body<8>(bk, a...))
+MKF_PERS_FN(kBodyModupSum4, void(ModUpSumArgs, int), modup_sum_body<4>(bk, a...))
+MKF_PERS_FN(kBodyModupSum8, void(ModUpSumArgs, int), modup_sum_body<8>(bk, a...))
+MKF_PERS_FN(kBodyCombine, std::remove_reference_t<decltype(moddown_combine_kernel)>, moddown_combine_body<true>(bk, a...))
+MKF_PERS_FN(kBodyKaratsuba, std::remove_reference_t<decltype(karatsuba_kernel)>, karatsuba_body(bk, a...))
+MKF_PERS_FN(kBodyRescaleSpread, std::remove_reference_t<decltype(rescale_spread_kernel)>, rescale_spread_body(bk, a...))
+MKF_PERS_FN(kBodyRescaleCombine, std::remove_reference_t<decltype(rescale_combine_kernel)>, rescale_combine_body(bk, a...))
+MKF_PERS_FN(kBodyReplicate, std::remove_reference_t<decltype(replicate_kernel)>, replicate_body(bk, a...))
+MKF_PERS_FN(kBodyIp111, void(IpArgs, const DevModulus *, int, int), ip_body<1, 1, 1, true>(bk, a...))
+MKF_PERS_FN(kBodyIp121, void(IpArgs, const DevModulus *, int, int), ip_body<1, 2, 1, true>(bk, a...))
+MKF_PERS_FN(kBodyIp221, void(IpArgs, const DevModulus *, int, int), ip_body<2, 2, 1, true>(bk, a...))
+MKF_PERS_FN(kBodyIp211, void(IpArgs, const DevModulus *, int, int), ip_body<2, 1, 1, true>(bk, a...))
+MKF_PERS_FN(kBodyIp112, void(IpArgs, const DevModulus *, int, int), ip_body<1, 1, 2, true>(bk, a...))
+MKF_PERS_FN(kBodyIp122, void(IpArgs, const DevModulus *, int, int), ip_body<1, 2, 2, true>(bk, a...))
+MKF_PERS_FN(kBodyIp222, void(IpArgs, const DevModulus *, int, int), ip_body<2, 2, 2, true>(bk, a...))
+MKF_PERS_FN(kBodyIp212, void(IpArgs, const DevModulus *, int, int), ip_body<2, 1, 2, true>(bk, a...))
+MKF_PERS_FN(kBodyCopyRows, void(CopyRowsArgs), copy_rows_body(bk, a...))
+MKF_PERS_FN(kBodyFill, void(FillArgs), fill_body(bk, a...))
+#undef MKF_PERS_FN
+
+MKF_DEV void pers_body(int kind, const VBlk &bk, const unsigned char *__restrict__ args) {
+#define MKF_PERS_CASE(KIND)                                                                        \
+    case KIND:                                                                                     \
+        pers_##KIND(bk, args);                                                                     \
+        break;
+    switch (kind) {
+        MKF_PERS_CASE(kBodyFwdCol6) MKF_PERS_CASE(kBodyFwdCol7) MKF_PERS_CASE(kBodyFwdCol8)
+        MKF_PERS_CASE(kBodyFwdRow7) MKF_PERS_CASE(kBodyFwdRow8)
+        MKF_PERS_CASE(kBodyInvCol6) MKF_PERS_CASE(kBodyInvCol7) MKF_PERS_CASE(kBodyInvCol8)
+        MKF_PERS_CASE(kBodyInvRow7) MKF_PERS_CASE(kBodyInvRow8)
+        MKF_PERS_CASE(kBodyDigitsCol6) MKF_PERS_CASE(kBodyDigitsCol7) MKF_PERS_CASE(kBodyDigitsCol8)
+        MKF_PERS_CASE(kBodyRowIp7) MKF_PERS_CASE(kBodyRowIp8)
+        MKF_PERS_CASE(kBodyDigitsPrep)
+        MKF_PERS_CASE(kBodyModup4) MKF_PERS_CASE(kBodyModup8)
+        MKF_PERS_CASE(kBodyModupSum4) MKF_PERS_CASE(kBodyModupSum8)
+        MKF_PERS_CASE(kBodyCombine) MKF_PERS_CASE(kBodyKaratsuba)
+        MKF_PERS_CASE(kBodyRescaleSpread) MKF_PERS_CASE(kBodyRescaleCombine)
+        MKF_PERS_CASE(kBodyReplicate) MKF_PERS_CASE(kBodyCopyRows) MKF_PERS_CASE(kBodyFill)
+        MKF_PERS_CASE(kBodyIp111) MKF_PERS_CASE(kBodyIp121) MKF_PERS_CASE(kBodyIp221)
+        MKF_PERS_CASE(kBodyIp211) MKF_PERS_CASE(kBodyIp112) MKF_PERS_CASE(kBodyIp122)
+        MKF_PERS_CASE(kBodyIp222) MKF_PERS_CASE(kBodyIp212)
+    default:
+        break;
+    }
+#undef MKF_PERS_CASE
+}
+
+MKF_DEV unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+MKF_DEV unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits until node dep has finished `need` items (thread 0 of the CTA).
+// Bounded by e.wait_ns of the global timer and by an iteration count; past
+// either, or once another wait has expired, it raises the error flag, notes
+// the first node that gave up, and returns.
+MKF_DEV void pers_wait(const PExec &e, unsigned node, int dep, unsigned need) {
+    const unsigned *c = e.ctl + kCtlDone0 + dep;
+    if (ld_acquire_u32(c) >= need) return;
+    const unsigned long long t0 = global_ns();
+    unsigned back = 32;
+    for (int it = 0;; ++it) {
+        if (ld_acquire_u32(c) >= need) return;
+        if (ld_acquire_u32(e.ctl + kCtlError) != 0u || global_ns() - t0 > e.wait_ns ||
+            it >= (1 << 24)) {
+            if (atomicExch(e.ctl + kCtlError, 1u) == 0u) atomicExch(e.ctl + kCtlStalled, node + 1u);
+            return;
+        }
+        __nanosleep(back);
+        back = back < 2048 ? 2 * back : back;
+    }
+}
+
+MKF_DEV VBlk pers_vblk(const PNode &nd, unsigned vb, unsigned t, unsigned bar, unsigned nt,
+                       uint64_t *sm) {
+    const unsigned x = vb % nd.gx, yz = vb / nd.gx;
+    return VBlk{make_uint3(x, yz % nd.gy, yz / nd.gy), make_uint3(nd.gx, nd.gy, nd.gz), t, bar, nt, sm};
+}
+
+__global__ void __launch_bounds__(kPersThreads, 2)
+    persistent_exec(PExec e, const unsigned char *__restrict__ blob) {
+    extern __shared__ __align__(16) uint64_t dsm[];
+    __shared__ unsigned s_item;
+    const unsigned tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(e.ctl + kCtlHead, 1u);
+        __syncthreads();
+        const unsigned i = s_item;
+        if (i >= e.nitems) return;
+        const PItem it = e.items[i];
+        const PNode nd = e.nodes[it.node];
+        if (tid == 0 && nd.dep >= 0) {
+            pers_wait(e, it.node, nd.dep, nd.dep_items);
+            __threadfence();
+        }
+        __syncthreads();
+        if (nd.threads == kPersThreads) {
+            pers_body(nd.kind, pers_vblk(nd, it.vb0, tid, 0u, kPersThreads, dsm), blob + nd.args);
+        } else {
+            // two 256-thread bodies, on named barriers 1 and 2
+            const unsigned h = tid >> 8, vb = it.vb0 + h;
+            if (vb < nd.nvb)
+                pers_body(nd.kind, pers_vblk(nd, vb, tid & 255u, 1u + h, 256u, dsm + h * nd.smem_words),
+                          blob + nd.args);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(e.ctl + kCtlDone0 + it.node, 1u);
+        }
+    }
+}
+
+int persistent_blocks(int device) {
+    static std::mutex mu;
+    static int per_dev[64] = {};
+    if (device < 0 || device >= 64) return 0;
+    std::lock_guard<std::mutex> g(mu);
+    if (!per_dev[device]) {
+        int prev = 0, sms = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaFuncSetAttribute(persistent_exec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kPersSmemBytes);
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persistent_exec, kPersThreads, kPersSmemBytes);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        per_dev[device] = nb * sms;
+        cudaSetDevice(prev);
+    }
+    return per_dev[device];
+}
+
+int launch_persistent(const PExec &e, int device, cudaStream_t st) {
+    const int blocks = persistent_blocks(device);
+    if (blocks <= 0) return 0;
+    note_launch();
+    persistent_exec<<<blocks, kPersThreads, kPersSmemBytes, st>>>(e, e.blob);
+    return cudaPeekAtLastError() == cudaSuccess ? blocks : 0;
+}
+
+// Host stubs of the kernels with bodies, for the launch recorder.
+static const bool g_ntt_bodies = [] {
+    const size_t tile = kTile, col = kColSmem / 8, rowip = kRowIpSmem / 8;
+    register_body((const void *)ntt_fwd_phase<6, true>, kBodyFwdCol6, kPhaseThreads, tile + 128);
+    register_body((const void *)ntt_fwd_phase<7, true>, kBodyFwdCol7, kPhaseThreads, tile + 256);
+    register_body((const void *)ntt_fwd_phase<8, true>, kBodyFwdCol8, kPhaseThreads, tile + 512);
+    register_body((const void *)ntt_fwd_phase<7, false>, kBodyFwdRow7, kPhaseThreads, tile);
+    register_body((const void *)ntt_fwd_phase<8, false>, kBodyFwdRow8, kPhaseThreads, tile);
+    register_body((const void *)ntt_inv_phase<6, true>, kBodyInvCol6, kPhaseThreads, tile);
+    register_body((const void *)ntt_inv_phase<7, true>, kBodyInvCol7, kPhaseThreads, tile);
+    register_body((const void *)ntt_inv_phase<8, true>, kBodyInvCol8, kPhaseThreads, tile);
+    register_body((const void *)ntt_inv_phase<7, false>, kBodyInvRow7, kPhaseThreads, tile);
+    register_body((const void *)ntt_inv_phase<8, false>, kBodyInvRow8, kPhaseThreads, tile);
+    register_body((const void *)ntt_fwd_digits_col<6>, kBodyDigitsCol6, kColThreads, col);
+    register_body((const void *)ntt_fwd_digits_col<7>, kBodyDigitsCol7, kColThreads, col);
+    register_body((const void *)ntt_fwd_digits_col<8>, kBodyDigitsCol8, kColThreads, col);
+    register_body((const void *)ntt_digits_row_ip<7>, kBodyRowIp7, kPhaseThreads, rowip);
+    register_body((const void *)ntt_digits_row_ip<8>, kBodyRowIp8, kPhaseThreads, rowip);
+    return true;
+}();
 
 } // namespace mkf
 

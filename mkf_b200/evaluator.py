@@ -372,10 +372,13 @@ class Batch:
     ("kklss", RelinearizationKeySet, op0, op1, out); outputs are shaped as for
     the single calls (see MKFEvaluator.output_level / Evaluator.MulRelinNew).
     fuse_keys: MKF-CKKS jobs that share a key bundle, flags and level run as
-    fused calls (each key read once per group; MKF_BATCH_FUSE_KEYS)."""
+    fused calls (each key read once per group; MKF_BATCH_FUSE_KEYS).
+    persistent: the whole plan runs as one launch of the persistent executor
+    (MKF_BATCH_PERSISTENT); check() then reports whether its bounded waits
+    all completed."""
 
     def __init__(self, params: Parameters, jobs, lanes: int = 8, graph: bool = True,
-                 fuse_keys: bool = False):
+                 fuse_keys: bool = False, persistent: bool = False, extra_flags: int = 0):
         self.params = params
         self._keep = list(jobs)  # handles must outlive the plan
         arr = (capi.Job * max(1, len(jobs)))()
@@ -393,7 +396,8 @@ class Batch:
             arr[i].a, arr[i].b, arr[i].out = left.handle, right.handle, out.handle
         self.jobs = arr
         h = ctypes.c_void_p()
-        flags = (capi.BATCH_GRAPH if graph else 0) | (capi.BATCH_FUSE_KEYS if fuse_keys else 0)
+        flags = (capi.BATCH_GRAPH if graph else 0) | (capi.BATCH_FUSE_KEYS if fuse_keys else 0) | \
+            (capi.BATCH_PERSISTENT if persistent else 0) | extra_flags
         st = capi.lib().mkf_batch_create(params.handle, arr, len(jobs), lanes, flags,
                                         ctypes.byref(h))
         capi.check(params.handle, st)
@@ -408,6 +412,11 @@ class Batch:
     @property
     def kernels(self) -> int:
         return int(capi.lib().mkf_batch_kernels(self.handle))
+
+    def check(self):
+        """Waits for the last launch; raises MKFError (MKF_ERR_TIMEOUT when a
+        persistent plan's bounded wait ran out)."""
+        capi.check(self.params.handle, capi.lib().mkf_batch_check(self.handle))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -182,3 +182,86 @@ def test_key_fused_batch_matches_single_calls(rings, graph, fuse_ip):
     b.close()
     for r in rings:
         autotune.set_tuning(r.P, fuse_ip=0)
+
+
+def _mkf_jobs(r14, r13):
+    """MKF-CKKS jobs of both rings (party counts, levels, compact and
+    materialized outputs) and their single calls."""
+    jobs, singles = _make_jobs(r14, r13)
+    keep = [i for i, j in enumerate(jobs) if j[0] == "mkf"]
+    return [jobs[i] for i in keep], [singles[i] for i in keep]
+
+
+@pytest.mark.parametrize("fuse_ip", [0, 1])
+@pytest.mark.parametrize("fuse_keys", [False, True])
+@pytest.mark.parametrize("graph", [False, True])
+def test_persistent_batch_matches_single_calls(rings, graph, fuse_keys, fuse_ip):
+    """MKF_BATCH_PERSISTENT: the whole plan is one launch of the persistent
+    executor; every output equals its single call bit for bit, on repeated
+    launches and after the operands change, on both inner-product forms."""
+    from mkf_b200 import autotune
+    r14, r13 = rings
+    orig = [autotune.get_tuning(r.P)["fuse_ip"] for r in rings]
+    for r in rings:
+        autotune.set_tuning(r.P, fuse_ip=fuse_ip)
+    jobs, singles = _mkf_jobs(r14, r13)
+    if fuse_keys:
+        for E, k, level, count, mat in [(r14.mkf[2], 2, 7, 5, True), (r13.mkf[3], 3, 4, 3, False)]:
+            ring = r14 if E.params is r14.P else r13
+            j, s = _fused_jobs(ring, E, k, level, count, mat)
+            jobs += j
+            singles += s
+    want = [f() for f in singles]
+    b = ev.Batch(r14.P, jobs, lanes=3, graph=graph, fuse_keys=fuse_keys, persistent=True)
+    assert b.statuses() == [0] * len(jobs)
+    assert b.kernels == 1
+    for rep in range(2):
+        b.launch()
+        b.check()
+        for i, j in enumerate(jobs):
+            assert np.array_equal(j[4].download(), want[i]), \
+                f"job {i} differs (graph={graph}, fuse_keys={fuse_keys}, fuse_ip={fuse_ip}, launch {rep})"
+    g = np.random.default_rng(7)
+    for j in jobs:
+        for op in (j[2], j[3]):
+            lit = r14.lit if op.params is r14.P else r13.lit
+            op.upload(_limbs(g, lit.q[: op.Level() + 1], lit.n, (op.n_comp,)))
+    want2 = [f() for f in singles]
+    b.launch()
+    b.check()
+    for i, j in enumerate(jobs):
+        assert np.array_equal(j[4].download(), want2[i]), f"job {i} differs after new operands"
+    b.close()
+    for r, f in zip(rings, orig):
+        autotune.set_tuning(r.P, fuse_ip=f)
+
+
+def test_persistent_batch_refuses_jobs_it_cannot_run(rings):
+    """KKLSS jobs launch kernels the executor has no body for: the plan is
+    refused, not run some other way."""
+    jobs, _ = _make_jobs(*rings)
+    kk = [j for j in jobs if j[0] == "kklss"]
+    with pytest.raises(capi.MKFError, match="persistent plan"):
+        ev.Batch(rings[0].P, kk, lanes=2, graph=False, persistent=True)
+
+
+def test_persistent_wait_bound_reports_timeout(rings):
+    """A wait that nothing completes (the test hook raises the last launch's
+    count by one) runs out after its bound: the launch ends, check() reports
+    MKF_ERR_TIMEOUT, and the context still runs a plan correctly after."""
+    r14, r13 = rings
+    jobs, singles = _mkf_jobs(r14, r13)
+    jobs, singles = jobs[:2], singles[:2]
+    want = [f() for f in singles]
+    bad = ev.Batch(r14.P, jobs, lanes=2, graph=False, persistent=True,
+                   extra_flags=capi.BATCH_TEST_STALL)
+    bad.launch()
+    with pytest.raises(capi.MKFError, match="MKF_ERR_TIMEOUT"):
+        bad.check()
+    bad.close()
+    good = ev.Batch(r14.P, jobs, lanes=2, graph=False, persistent=True)
+    good.launch()
+    good.check()
+    for i, j in enumerate(jobs):
+        assert np.array_equal(j[4].download(), want[i])
+    good.close()
