@@ -106,6 +106,7 @@ struct PlanRecorder final : LaunchRecorder {
         n.gx = g.x;
         n.gy = g.y;
         n.gz = g.z;
+        n.vpi = 1;
         n.items = threads == kPersThreads ? n.nvb : (n.nvb + 1) / 2;
         n.dep = -1;
         const size_t off = (blob.size() + 15) & ~size_t(15);
@@ -254,6 +255,16 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
     if (stray)
         return fail(b->ctx, MKF_ERR_INVALID_ARG,
                     "persistent plan: the jobs issue operations the executor cannot record");
+    // Items: a launch of many small blocks is taken a run of blocks at a
+    // time (at least 4 items per executor CTA, at most 64 blocks per item), so
+    // that the queue traffic and barriers of an item stay small beside its work.
+    const unsigned ncta = (unsigned)persistent_blocks(b->device);
+    for (auto &ln : rec.lanes)
+        for (PNode &n : ln) {
+            const unsigned slots = n.threads == kPersThreads ? n.nvb : (n.nvb + 1) / 2;
+            n.vpi = std::max(1u, std::min(64u, slots / (4 * ncta)));
+            n.items = (slots + n.vpi - 1) / n.vpi;
+        }
     std::vector<PNode> nodes;
     std::vector<PItem> items;
     std::vector<int> prev(rec.lanes.size(), -1);
@@ -267,7 +278,7 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
             n.dep_items = prev[l] >= 0 ? nodes[prev[l]].items : 0;
             const unsigned id = (unsigned)nodes.size();
             prev[l] = (int)id;
-            const unsigned per = n.threads == kPersThreads ? 1u : 2u;
+            const unsigned per = (n.threads == kPersThreads ? 1u : 2u) * n.vpi;
             for (unsigned i = 0; i < n.items; ++i) items.push_back(PItem{id, i * per});
             nodes.push_back(n);
         }

@@ -1562,13 +1562,22 @@ __global__ void __launch_bounds__(kPersThreads, 2)
         }
         __syncthreads();
         if (nd.threads == kPersThreads) {
-            pers_body(nd.kind, pers_vblk(nd, it.vb0, tid, 0u, kPersThreads, dsm), blob + nd.args);
+            for (unsigned j = 0; j < nd.vpi; ++j) {
+                const unsigned vb = it.vb0 + j;
+                if (vb >= nd.nvb) break;
+                if (j) __syncthreads(); // the previous block's shared memory reads are done
+                pers_body(nd.kind, pers_vblk(nd, vb, tid, 0u, kPersThreads, dsm), blob + nd.args);
+            }
         } else {
             // two 256-thread bodies, on named barriers 1 and 2
-            const unsigned h = tid >> 8, vb = it.vb0 + h;
-            if (vb < nd.nvb)
+            const unsigned h = tid >> 8;
+            for (unsigned j = 0; j < nd.vpi; ++j) {
+                const unsigned vb = it.vb0 + 2 * j + h;
+                if (vb >= nd.nvb) break;
+                if (j) asm volatile("bar.sync %0, 256;" ::"r"(1u + h) : "memory");
                 pers_body(nd.kind, pers_vblk(nd, vb, tid & 255u, 1u + h, 256u, dsm + h * nd.smem_words),
                           blob + nd.args);
+            }
         }
         __syncthreads();
         if (tid == 0) {

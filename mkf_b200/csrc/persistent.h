@@ -38,7 +38,8 @@ struct PNode {
     int threads;         // 512, or 256 (two bodies per CTA)
     unsigned nvb;        // virtual blocks: gx * gy * gz
     unsigned gx, gy, gz; // the launch's grid
-    unsigned items;      // queue items: nvb (512) or ceil(nvb / 2) (256)
+    unsigned vpi;        // virtual blocks per item and body slot
+    unsigned items;      // queue items: ceil(nvb / vpi) (512), ceil(nvb / (2 vpi)) (256)
     int dep;             // the node this one waits for (-1: none)
     unsigned dep_items;  // how many items of dep must have finished
     unsigned args;       // byte offset of the argument record in the blob
@@ -46,7 +47,9 @@ struct PNode {
     unsigned smem_words; // shared memory words of one body (offset of the second)
 };
 struct PItem {
-    unsigned node, vb0; // the node and its first virtual block
+    unsigned node, vb0; // the node and its first virtual block; a 512-thread
+                        // item runs vb0 .. vb0+vpi-1, the halves of a
+                        // 256-thread item vb0+h, vb0+h+2, ... (h = 0, 1)
 };
 // Control words: [0] queue head, [1] error flag, [2] first node whose wait
 // expired + 1, [3] unused, then one finished-item counter per node.
