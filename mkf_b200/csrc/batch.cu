@@ -170,6 +170,8 @@ struct mkf_batch {
     unsigned nitems = 0, nnodes = 0;
     unsigned long long wait_ns = 0;
     cudaStream_t last_stream = nullptr;
+    // the lane scratch buffers a graph or persistent plan recorded addresses in
+    std::vector<std::shared_ptr<ScratchBuf>> held;
 };
 
 namespace {
@@ -430,6 +432,7 @@ mkf_status mkf_batch_create(mkf_ctx *ctx, mkf_job *jobs, int n, int lanes, int f
             cudaSetDevice(kv.first->c.device);
             Workspace *ws = workspace(kv.first, ctx_lane(kv.first, l));
             if (!ws->reserve(kv.second)) return fail(ctx, MKF_ERR_OOM, "lane workspace allocation failed");
+            if (flags & (MKF_BATCH_GRAPH | MKF_BATCH_PERSISTENT)) b->held.push_back(ws->hold());
         }
     }
     for (mkf_ctx *jc : ctxs) ntt_prepare(jc->c);

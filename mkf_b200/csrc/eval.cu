@@ -10,12 +10,12 @@
 
 namespace mkf {
 
-Workspace::~Workspace() {
-    if (buf) {
+ScratchBuf::~ScratchBuf() {
+    if (p) {
         int prev = 0;
         cudaGetDevice(&prev);
         cudaSetDevice(device);
-        cudaFree(buf);
+        cudaFree(p); // waits for pending work on the device
         cudaSetDevice(prev);
     }
 }
@@ -25,15 +25,21 @@ bool Workspace::reserve(size_t words) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
-    if (buf) cudaFree(buf); // cudaFree waits for pending work on the device
+    // the current buffer goes now unless a plan still holds it
+    cur.reset();
     buf = nullptr;
     cap_words = 0;
-    size_t w = words + words / 8 + 1024;
-    bool ok = cudaMalloc(&buf, w * 8) == cudaSuccess;
-    if (ok)
+    const size_t w = words + words / 8 + 1024;
+    auto nb = std::make_shared<ScratchBuf>();
+    nb->device = device;
+    const bool ok = cudaMalloc(&nb->p, w * 8) == cudaSuccess;
+    if (ok) {
+        cur = nb;
+        buf = nb->p;
         cap_words = w;
-    else
-        buf = nullptr;
+    } else {
+        nb->p = nullptr;
+    }
     cudaSetDevice(prev);
     return ok;
 }

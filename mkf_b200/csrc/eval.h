@@ -1,6 +1,7 @@
 // Multi-key mult+relin algorithms on device-resident operands.
 #pragma once
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -33,14 +34,25 @@ struct Arena {
     }
 };
 
-// Per-stream scratch memory.
+// One device allocation, freed when its last holder lets go.
+struct ScratchBuf {
+    int device = 0;
+    uint64_t *p = nullptr;
+    ~ScratchBuf();
+};
+
+// Per-stream scratch memory.  A plan that recorded addresses in the buffer
+// (a captured graph, a persistent plan) holds the buffer (hold()), so a later
+// growth of the workspace leaves that plan's buffer in place; the workspace
+// then moves on to a new, larger one.
 struct Workspace {
     int device = 0;
     uint64_t *buf = nullptr;
     size_t cap_words = 0;
-    ~Workspace();
+    std::shared_ptr<ScratchBuf> cur;
     // grows the buffer (never during stream capture); returns false on OOM
     bool reserve(size_t words);
+    std::shared_ptr<ScratchBuf> hold() const { return cur; }
     Arena arena() const {
         Arena a;
         a.base = buf;

@@ -265,3 +265,28 @@ def test_persistent_wait_bound_reports_timeout(rings):
     for i, j in enumerate(jobs):
         assert np.array_equal(j[4].download(), want[i])
     good.close()
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_plan_keeps_its_scratch_when_a_later_plan_grows_the_lanes(rings, persistent):
+    """A graph (or persistent) plan records addresses in its lanes' scratch;
+    a later plan on the same lanes that needs more scratch must not free it:
+    the first plan, launched again after the second was made, still gives
+    the single-call results."""
+    r14, r13 = rings
+    small, small_want = _mkf_jobs(r14, r13)
+    small, small_want = small[:3], [f() for f in small_want[:3]]
+    a = ev.Batch(r14.P, small, lanes=2, graph=True, persistent=persistent)
+    # a wider fused group than any plan before it made on these lanes
+    big, big_singles = _fused_jobs(r14, r14.mkf[3], 3, 7, 10 if persistent else 8, True)
+    big_want = [f() for f in big_singles]
+    b = ev.Batch(r14.P, big, lanes=2, graph=True, fuse_keys=True, persistent=persistent)
+    for plan, jobs, want in [(a, small, small_want), (b, big, big_want), (a, small, small_want)]:
+        for j in jobs:
+            j[4].upload(np.zeros_like(j[4].download()))
+        plan.launch()
+        plan.check()
+        for i, j in enumerate(jobs):
+            assert np.array_equal(j[4].download(), want[i]), f"job {i} differs"
+    a.close()
+    b.close()
