@@ -890,9 +890,17 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
             p_ms = timed(plain_sub, reps)
             bb = ev.Batch(P0, sub, lanes=lanes, graph=True, fuse_keys=fuse, persistent=pers)
             b_ms = timed(lambda: bb.launch(cs), reps)
+            bb.check()
             bb.close()
             buckets[f"{name}_k{kb}"] = {"products": len(sub), "plain_ms": p_ms, "batched_ms": b_ms,
                                         "batched_over_plain": p_ms / b_ms}
+            if "persistent" in forms and not pers:
+                # the bucket as one persistent launch, beside the chosen form
+                bp = ev.Batch(P0, sub, lanes=lanes, graph=True, fuse_keys=fuse, persistent=True)
+                pp_ms = timed(lambda: bp.launch(cs), reps)
+                bp.check()
+                bp.close()
+                buckets[f"{name}_k{kb}"]["persistent_ms"] = pp_ms
     res = {"workload": f"{n} MK-CKKS mult+relin+rescale+materialize products, k uniform over "
                        "{2,4,8,16}, logN uniform over {14 (S14: 55b+7x40b, P 2x45b), "
                        "15 (S15: 60b+15x50b, P 4x60b)}, level uniform over [1,L]",
