@@ -800,11 +800,16 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
     import torch
     from mkf_b200 import capi, params
     from mkf_b200 import evaluator as ev
+    from mkf_b200 import autotune
     g = np.random.Generator(np.random.PCG64(777 + rank))
-    rings = {}
+    rings, splits = {}, {}
     for name in ("S14", "S15"):
         lit = params.get("ckks", name)
-        P = ev.Parameters(lit, "ckks", device=local)
+        # the NTT phase split of the ring, by timing a k = 8 top-level product
+        rl, split_ms = autotune.tune_split(lit, "ckks", 8, device=local, reps=3)
+        splits[name] = {"row_log": rl, "col_log": lit.log_n - rl,
+                        "ms_per_product": {str(k_): v for k_, v in split_ms.items()}}
+        P = ev.Parameters(lit, "ckks", device=local, ntt_row_log=rl)
         nQ, nP, N = len(lit.q), len(lit.p), lit.n
         qmin = min(min(lit.q), min(lit.p))
         beta = (nQ + nP - 1) // nP
@@ -911,6 +916,7 @@ def run_mix(a, local, rank, barrier, max_over_ranks):
                        "kernels_per_launch": kernels},
            "batched_over_plain": plain_ms / batch_ms,
            "autotune_plan_ms": tried,
+           "ntt_split": splits,
            "buckets": buckets,
            "mix": {f"k{k}": sum(1 for s in shapes if s[1] == k) for k in (2, 4, 8, 16)}}
     b.close()

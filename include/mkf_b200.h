@@ -65,6 +65,13 @@ typedef struct mkf_params_desc {
     double scale;         /* CKKS default scale */
     uint64_t t;           /* BFV plaintext modulus */
     int device;           /* CUDA device ordinal */
+    /* NTT split (logN 13-16): the transform runs as a column phase of
+     * logN - ntt_row_log stages and a row phase of ntt_row_log stages, each
+     * radix-8 passes plus one pass of radix 2^(stages mod 3).  0 = the
+     * default ceil(logN/2); logN 14 also takes 8 (6 + 8), logN 15 also 7
+     * (8 + 7).  The result is the same transform either way; the split only
+     * changes the kernels' shapes (mkf_b200.autotune picks it by timing). */
+    int ntt_row_log;
 } mkf_params_desc;
 
 /* Creates a context (moduli, NTT and basis-extension tables in HBM).

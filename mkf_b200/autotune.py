@@ -11,8 +11,13 @@ The choices (mkf_tuning) never change the words computed, only the time:
   column tile share its limb walk, ceil(limbs / col_split) limbs each);
 * ``modup_chunk``: target limbs per thread of the party-summed ModUp.
 
-The NTT's radix is fixed at 8 (three butterfly stages per pass on eight
-words held in registers), its phase split by the ring degree.
+The NTT runs as a column phase and a row phase; each phase is radix-8
+passes (three butterfly stages on eight words held in registers) plus one
+pass of radix 2^(stages mod 3), so the phase split sets the radix
+composition: at logN 15, 7 + 8 stages (8*8*2 and 8*8*4) or 8 + 7; at
+logN 14, 7 + 7 or 6 + 8.  The split is a context creation choice
+(Parameters(..., ntt_row_log=)), picked by ``tune_split``, which times one
+product on a context of each split.
 
 The tuner times a product per candidate with CUDA events (after a warm-up)
 in a coordinate descent over the axes (each axis swept with the others held
@@ -94,6 +99,50 @@ def descend(axes: Dict[str, Iterable], time_fn: Callable[[dict], float], start: 
             cur[ax] = best_v
     best_key = min(table, key=table.get)
     return json.loads(best_key), table
+
+
+def split_options(log_n: int) -> List[int]:
+    """Row-phase stage counts (ntt_row_log) the kernels are built for at
+    log_n, the default first; [] below logN 13 (one tile holds a limb)."""
+    return {13: [7], 14: [7, 8], 15: [8, 7], 16: [8]}.get(log_n, [])
+
+
+def tune_split(literal, scheme: str, k: int, level: Optional[int] = None, device: int = 0,
+               reps: int = 4) -> Tuple[int, Dict[int, float]]:
+    """Times one MKF mult+relin(+rescale) of k parties on a context of each
+    NTT split of the ring (random keys and operands, default launch choices
+    otherwise) and returns (the fastest ntt_row_log, {row_log: ms})."""
+    import torch
+    from . import evaluator as ev
+    opts = split_options(literal.log_n)
+    if len(opts) < 2:
+        return (opts[0] if opts else 0), {}
+    level = literal.max_level if level is None else level
+    g = np.random.default_rng(11)
+    qmin = min(min(literal.q), min(literal.p))
+    nQ, nP, N = len(literal.q), len(literal.p), literal.n
+    beta = (nQ + nP - 1) // nP
+    kimg = g.integers(0, qmin, size=(beta, 2, nQ + nP, N), dtype=np.uint64)
+    cimg = [g.integers(0, qmin, size=(k + 1, level + 1, N), dtype=np.uint64) for _ in range(2)]
+    ckks = scheme == "ckks"
+    table = {}
+    for rl in opts:
+        P = ev.Parameters(literal, scheme, device=device, ntt_row_log=rl)
+        E = ev.MKFEvaluator(P, ev.MKFKeySet(P, [kimg] * k, kimg))
+        left, right = (ev.Ciphertext.from_array(P, c, ckks, scale=literal.scale) for c in cimg)
+        out = ev.Ciphertext(P, k + 1, E.output_level(left, right, ckks), ckks)
+        st = torch.cuda.Stream(device=device)
+        cs = ctypes.c_void_p(st.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        E.MulRelin(left, right, out, rescale=ckks, materialize=True, stream=cs)  # warm-up
+        e0.record(st)
+        for _ in range(reps):
+            E.MulRelin(left, right, out, rescale=ckks, materialize=True, stream=cs)
+        e1.record(st)
+        e1.synchronize()
+        table[rl] = e0.elapsed_time(e1) / reps
+        del out, left, right, E, P
+    return min(table, key=table.get), table
 
 
 def _cache_key(params, k: int, level: int) -> str:

@@ -53,6 +53,7 @@ class ParamsDesc(ctypes.Structure):
         ("p", u64p), ("n_p", ctypes.c_int),
         ("q_mul", u64p), ("n_q_mul", ctypes.c_int),
         ("scale", ctypes.c_double), ("t", ctypes.c_uint64), ("device", ctypes.c_int),
+        ("ntt_row_log", ctypes.c_int),
     ]
 
 

@@ -389,7 +389,7 @@ mkf_status mkf_ctx_create(const mkf_params_desc *d, mkf_ctx **out) {
     if (!ctx) return MKF_ERR_OOM;
     std::string e = ctx->c.init(d->scheme, d->log_n, d->q, d->n_q, d->p, d->n_p, d->q_mul,
                                 d->scheme == MKF_SCHEME_BFV ? d->n_q_mul : 0, d->scale, d->t,
-                                d->device);
+                                d->device, d->ntt_row_log);
     if (!e.empty()) {
         delete ctx;
         return e.find("device") != std::string::npos ? MKF_ERR_CUDA : MKF_ERR_INVALID_ARG;

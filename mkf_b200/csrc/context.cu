@@ -247,7 +247,7 @@ ModUpTab Context::make_modup(const std::vector<int> &src, const std::vector<int>
 
 std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, const uint64_t *p,
                           int np, const uint64_t *qm, int nqm, double scale_, uint64_t t_,
-                          int device_) {
+                          int device_, int row_log) {
     scheme = scheme_;
     logN = logN_;
     N = 1 << logN;
@@ -279,13 +279,19 @@ std::string Context::init(int scheme_, int logN_, const uint64_t *q, int nq, con
     if (nQM && nQM != nQ) return "BFV requires len(QMul) == len(Q)";
     if (cudaSetDevice(device) != cudaSuccess) return "cudaSetDevice failed";
 
-    // NTT split
+    // NTT split: row stages (contiguous rows of 2^n2 words) and column
+    // stages; each phase runs radix-8 passes plus one of radix 2^(n mod 3)
     if (logN <= 12) {
         n1 = logN;
         n2 = 0;
     } else {
-        n2 = (logN + 1) / 2; // row stages (contiguous rows of 2^n2 words)
-        n1 = logN - n2;      // column stages
+        n2 = row_log ? row_log : (logN + 1) / 2;
+        n1 = logN - n2;
+        const int key = n1 * 16 + n2;
+        if (key != 6 * 16 + 7 && key != 7 * 16 + 7 && key != 6 * 16 + 8 && key != 7 * 16 + 8 &&
+            key != 8 * 16 + 7 && key != 8 * 16 + 8)
+            return "NTT split " + std::to_string(n1) + "+" + std::to_string(n2) +
+                   " not built for logN " + std::to_string(logN);
     }
     const int S1 = 1 << n1;
 

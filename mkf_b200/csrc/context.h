@@ -138,8 +138,10 @@ class Context {
     }
 
     // build everything; returns "" on success or an error message
+    // row_log: row stages of the NTT split (0: ceil(logN / 2))
     std::string init(int scheme, int logN, const uint64_t *q, int nq, const uint64_t *p, int np,
-                     const uint64_t *qm, int nqm, double scale, uint64_t t, int device);
+                     const uint64_t *qm, int nqm, double scale, uint64_t t, int device,
+                     int row_log = 0);
 
   private:
     ModUpTab make_modup(const std::vector<int> &src, const std::vector<int> &tgt);

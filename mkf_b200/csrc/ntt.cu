@@ -1047,11 +1047,14 @@ static void launch_split(const Context &c, const LimbSet &ls, int npolys, cudaSt
             else
                 PdlLaunch(grid, block, 0, st)(ntt_fwd_tile, b);
         } else {
-            switch (c.logN) {
-            case 13: launch_phases<6, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
-            case 14: launch_phases<7, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
-            case 15: launch_phases<7, 8>(b, np, ls.limbs, st, inverse, c, bytes); break;
-            case 16: launch_phases<8, 8>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            // the context's split: column stages n1, row stages n2
+            switch (c.n1 * 16 + c.n2) {
+            case 6 * 16 + 7: launch_phases<6, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            case 7 * 16 + 7: launch_phases<7, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            case 6 * 16 + 8: launch_phases<6, 8>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            case 7 * 16 + 8: launch_phases<7, 8>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            case 8 * 16 + 7: launch_phases<8, 7>(b, np, ls.limbs, st, inverse, c, bytes); break;
+            case 8 * 16 + 8: launch_phases<8, 8>(b, np, ls.limbs, st, inverse, c, bytes); break;
             default: break;
             }
         }
@@ -1236,9 +1239,9 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
     // the column pass: split at whole polynomials so that grid.y stays below 2^16
     const int max_polys = std::max(src.ndigits, (65535 / limbs) / src.ndigits * src.ndigits);
     note_launch(1);
-    switch (c.logN) {
+    switch (c.n1 * 16 + c.n2) {
 #define MKF_DIGITS_IP_CASE(LN, L1G, L2G)                                                           \
-    case LN: {                                                                                     \
+    case (L1G) * 16 + (L2G): {                                                                                     \
         for (int p0 = 0; p0 < np; p0 += max_polys) {                                               \
             const int npp = std::min(max_polys, np - p0);                                          \
             NttArgs b = a;                                                                         \
@@ -1267,6 +1270,8 @@ void ntt_forward_digits_ip(const Context &c, const DigitSrc &src0, uint64_t *dig
         MKF_DIGITS_IP_CASE(14, 7, 7)
         MKF_DIGITS_IP_CASE(15, 7, 8)
         MKF_DIGITS_IP_CASE(16, 8, 8)
+        MKF_DIGITS_IP_CASE(14, 6, 8)
+        MKF_DIGITS_IP_CASE(15, 8, 7)
 #undef MKF_DIGITS_IP_CASE
     default: break;
     }
@@ -1327,9 +1332,9 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
         const double bytes_row = 16.0 * c.N * npp * (limbs - own);
         dim3 block(kPhaseThreads);
         note_launch(2);
-        switch (c.logN) {
+        switch (c.n1 * 16 + c.n2) {
 #define MKF_DIGITS_CASE(LN, L1G, L2G)                                                              \
-    case LN: {                                                                                     \
+    case (L1G) * 16 + (L2G): {                                                                                     \
         dim3 g1((1 << L2G) / (kColWords >> L1G), npp, c.tune.col_split), g2((1 << L1G) / (kTile >> L2G), npp * limbs); \
         {                                                                                          \
             ProfScope ps(c, PK_DIGITS_COL, st, bytes_col);                                         \
@@ -1344,6 +1349,8 @@ void ntt_forward_digits(const Context &c, const DigitSrc &src, uint64_t *out, in
             MKF_DIGITS_CASE(14, 7, 7)
             MKF_DIGITS_CASE(15, 7, 8)
             MKF_DIGITS_CASE(16, 8, 8)
+            MKF_DIGITS_CASE(14, 6, 8)
+            MKF_DIGITS_CASE(15, 8, 7)
 #undef MKF_DIGITS_CASE
         default: break;
         }

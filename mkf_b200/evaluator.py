@@ -28,9 +28,12 @@ from .params import ParametersLiteral
 
 
 class Parameters:
-    """A parameter literal instantiated on one GPU (tables resident in HBM)."""
+    """A parameter literal instantiated on one GPU (tables resident in HBM).
+    ntt_row_log: row stages of the NTT split (0: ceil(logN/2); logN 14 also
+    takes 8, logN 15 also 7); the transform's results do not depend on it."""
 
-    def __init__(self, literal: ParametersLiteral, scheme: str, device: int = 0):
+    def __init__(self, literal: ParametersLiteral, scheme: str, device: int = 0,
+                 ntt_row_log: int = 0):
         L = capi.lib()
         self.literal = literal
         self.scheme = scheme.lower()
@@ -48,6 +51,8 @@ class Parameters:
         d.scale = literal.scale
         d.t = literal.t
         d.device = device
+        d.ntt_row_log = ntt_row_log
+        self.ntt_row_log = ntt_row_log
         h = ctypes.c_void_p()
         st = L.mkf_ctx_create(ctypes.byref(d), ctypes.byref(h))
         if st != capi.OK:

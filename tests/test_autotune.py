@@ -48,3 +48,16 @@ def test_search_keeps_each_candidates_best_time():
     times = iter([5.0, 1.0, 9.0, 2.0])  # sweep 1: a=5, b=1; sweep 2: a=9, b=2
     best, table = autotune.search([{"x": 0}, {"x": 1}], lambda c: next(times))
     assert best == {"x": 1} and table['{"x": 0}'] == 5.0 and table['{"x": 1}'] == 1.0
+
+
+def test_split_options_are_the_built_phase_pairs():
+    """The NTT splits the kernels are built for: the default (ceil(logN/2)
+    row stages) first, then the other split where one exists."""
+    assert autotune.split_options(12) == []
+    assert autotune.split_options(13) == [7]
+    assert autotune.split_options(14) == [7, 8]
+    assert autotune.split_options(15) == [8, 7]
+    assert autotune.split_options(16) == [8]
+    for log_n in (13, 14, 15, 16):
+        for rl in autotune.split_options(log_n):
+            assert 6 <= log_n - rl <= 8 and 7 <= rl <= 8
