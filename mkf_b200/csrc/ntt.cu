@@ -1524,24 +1524,52 @@ MKF_DEV unsigned long long global_ns() {
     return t;
 }
 
-// Waits until node dep has finished `need` items (thread 0 of the CTA).
-// Bounded by e.wait_ns of the global timer and by an iteration count; past
-// either, or once another wait has expired, it raises the error flag, notes
-// the first node that gave up, and returns.
-MKF_DEV void pers_wait(const PExec &e, unsigned node, int dep, unsigned need) {
-    const unsigned *c = e.ctl + kCtlDone0 + dep;
-    if (ld_acquire_u32(c) >= need) return;
-    const unsigned long long t0 = global_ns();
+// Claims for this CTA (thread 0) the next item of some lane whose launch may
+// start: the launch before it in the lane has finished all its items.  The
+// lanes are scanned from the one this CTA last took an item from; a claim is
+// a compare-and-swap of the lane's head, so an item is run once and only
+// once it is ready (no CTA ever holds an item it must wait for).  Returns
+// the item, or kNoItem when every lane is finished.  Waiting for ready work
+// is bounded by e.wait_ns of the global timer and an iteration count; past
+// either, or once another CTA has given up, it raises the error flag, notes
+// the node it was waiting for, and returns kNoItem.
+constexpr unsigned kNoItem = 0xffffffffu;
+MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
+    unsigned *heads = e.ctl + kCtlDone0 + e.nnodes;
+    unsigned long long t0 = 0;
     unsigned back = 32;
     for (int it = 0;; ++it) {
-        if (ld_acquire_u32(c) >= need) return;
-        if (ld_acquire_u32(e.ctl + kCtlError) != 0u || global_ns() - t0 > e.wait_ns ||
-            it >= (1 << 24)) {
-            if (atomicExch(e.ctl + kCtlError, 1u) == 0u) atomicExch(e.ctl + kCtlStalled, node + 1u);
-            return;
+        if (ld_acquire_u32(e.ctl + kCtlError) != 0u) return kNoItem;
+        unsigned finished = 0, waiting = 0;
+        for (unsigned j = 0; j < e.nlanes; ++j) {
+            const unsigned l = lane0 + j < e.nlanes ? lane0 + j : lane0 + j - e.nlanes;
+            const uint2 r = e.lanes[l];
+            unsigned h = ld_acquire_u32(heads + l);
+            while (h < r.y) {
+                const unsigned node = e.items[h].node;
+                const int dep = e.nodes[node].dep;
+                if (dep >= 0 && ld_acquire_u32(e.ctl + kCtlDone0 + dep) < e.nodes[node].dep_items) {
+                    waiting = node + 1u;
+                    break;
+                }
+                const unsigned prev = atomicCAS(heads + l, h, h + 1u);
+                if (prev == h) {
+                    lane0 = l;
+                    return h;
+                }
+                h = prev; // another CTA took it: look at the new head
+            }
+            if (h >= r.y) ++finished;
+        }
+        if (finished == e.nlanes) return kNoItem;
+        if (t0 == 0) {
+            t0 = global_ns();
+        } else if (global_ns() - t0 > e.wait_ns || it >= (1 << 24)) {
+            if (atomicExch(e.ctl + kCtlError, 1u) == 0u) atomicExch(e.ctl + kCtlStalled, waiting);
+            return kNoItem;
         }
         __nanosleep(back);
-        back = back < 2048 ? 2 * back : back;
+        back = back < 1024 ? 2 * back : back;
     }
 }
 
@@ -1556,18 +1584,17 @@ __global__ void __launch_bounds__(kPersThreads, 2)
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ unsigned s_item;
     const unsigned tid = threadIdx.x;
+    unsigned lane0 = e.nlanes ? blockIdx.x % e.nlanes : 0u; // thread 0's scan start
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(e.ctl + kCtlHead, 1u);
-        __syncthreads();
-        const unsigned i = s_item;
-        if (i >= e.nitems) return;
-        const PItem it = e.items[i];
-        const PNode nd = e.nodes[it.node];
-        if (tid == 0 && nd.dep >= 0) {
-            pers_wait(e, it.node, nd.dep, nd.dep_items);
-            __threadfence();
+        if (tid == 0) {
+            s_item = pers_claim(e, lane0);
+            __threadfence(); // the claimed item's inputs (acquired above) before the body's loads
         }
         __syncthreads();
+        const unsigned i = s_item;
+        if (i == kNoItem) return;
+        const PItem it = e.items[i];
+        const PNode nd = e.nodes[it.node];
         if (nd.threads == kPersThreads) {
             for (unsigned j = 0; j < nd.vpi; ++j) {
                 const unsigned vb = it.vb0 + j;
