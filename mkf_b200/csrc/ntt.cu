@@ -1543,10 +1543,12 @@ MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
         unsigned finished = 0, waiting = 0;
         for (unsigned j = 0; j < e.nlanes; ++j) {
             const unsigned l = lane0 + j < e.nlanes ? lane0 + j : lane0 + j - e.nlanes;
+            // the lane's items are [r.x, r.y); its head counts the ones claimed
             const uint2 r = e.lanes[l];
+            const unsigned len = r.y - r.x;
             unsigned h = ld_acquire_u32(heads + l);
-            while (h < r.y) {
-                const unsigned node = e.items[h].node;
+            while (h < len) {
+                const unsigned node = e.items[r.x + h].node;
                 const int dep = e.nodes[node].dep;
                 if (dep >= 0 && ld_acquire_u32(e.ctl + kCtlDone0 + dep) < e.nodes[node].dep_items) {
                     waiting = node + 1u;
@@ -1555,11 +1557,11 @@ MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
                 const unsigned prev = atomicCAS(heads + l, h, h + 1u);
                 if (prev == h) {
                     lane0 = l;
-                    return h;
+                    return r.x + h;
                 }
                 h = prev; // another CTA took it: look at the new head
             }
-            if (h >= r.y) ++finished;
+            if (h >= len) ++finished;
         }
         if (finished == e.nlanes) return kNoItem;
         if (t0 == 0) {
