@@ -1524,15 +1524,36 @@ MKF_DEV unsigned long long global_ns() {
     return t;
 }
 
-// Claims for this CTA (thread 0) the next item of some lane whose launch may
-// start: the launch before it in the lane has finished all its items.  The
-// lanes are scanned from the one this CTA last took an item from; a claim is
-// a compare-and-swap of the lane's head, so an item is run once and only
-// once it is ready (no CTA ever holds an item it must wait for).  Returns
-// the item, or kNoItem when every lane is finished.  Waiting for ready work
-// is bounded by e.wait_ns of the global timer and an iteration count; past
-// either, or once another CTA has given up, it raises the error flag, notes
-// the node it was waiting for, and returns kNoItem.
+// Waits until node dep has finished `need` items (thread 0 of the CTA).
+// Bounded by e.wait_ns of the global timer and by an iteration count; past
+// either, or once another wait has run out, it raises the error flag, notes
+// the node that gave up, and returns.
+MKF_DEV void pers_wait(const PExec &e, unsigned node, int dep, unsigned need) {
+    const unsigned *c = e.ctl + kCtlDone0 + dep;
+    if (ld_acquire_u32(c) >= need) return;
+    const unsigned long long t0 = global_ns();
+    unsigned back = 32;
+    for (int it = 0;; ++it) {
+        if (ld_acquire_u32(c) >= need) return;
+        if (ld_acquire_u32(e.ctl + kCtlError) != 0u || global_ns() - t0 > e.wait_ns ||
+            it >= (1 << 24)) {
+            if (atomicExch(e.ctl + kCtlError, 1u) == 0u) atomicExch(e.ctl + kCtlStalled, node + 1u);
+            return;
+        }
+        __nanosleep(back);
+        back = back < 2048 ? 2 * back : back;
+    }
+}
+
+// Claims for this CTA (thread 0) the next item of a lane whose head launch
+// may start (the launch before it in the lane has finished all its items):
+// the lanes are scanned from the one this CTA last took an item from, and
+// the claim is an atomic add on that lane's head, so it may land on the
+// next launch of the lane, which the caller then waits for (pers_wait).  A
+// lane whose head launch cannot start is passed over, so no CTA holds an
+// item behind another lane's unfinished work.  Returns the item, or kNoItem
+// when every lane is finished.  When no lane can start, the wait is bounded
+// like pers_wait's.
 constexpr unsigned kNoItem = 0xffffffffu;
 MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
     unsigned *heads = e.ctl + kCtlDone0 + e.nnodes;
@@ -1546,22 +1567,22 @@ MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
             // the lane's items are [r.x, r.y); its head counts the ones claimed
             const uint2 r = e.lanes[l];
             const unsigned len = r.y - r.x;
-            unsigned h = ld_acquire_u32(heads + l);
-            while (h < len) {
-                const unsigned node = e.items[r.x + h].node;
-                const int dep = e.nodes[node].dep;
-                if (dep >= 0 && ld_acquire_u32(e.ctl + kCtlDone0 + dep) < e.nodes[node].dep_items) {
-                    waiting = node + 1u;
-                    break;
-                }
-                const unsigned prev = atomicCAS(heads + l, h, h + 1u);
-                if (prev == h) {
-                    lane0 = l;
-                    return r.x + h;
-                }
-                h = prev; // another CTA took it: look at the new head
+            const unsigned h = ld_acquire_u32(heads + l);
+            if (h >= len) {
+                ++finished;
+                continue;
             }
-            if (h >= len) ++finished;
+            const unsigned node = e.items[r.x + h].node;
+            const int dep = e.nodes[node].dep;
+            if (dep >= 0 && ld_acquire_u32(e.ctl + kCtlDone0 + dep) < e.nodes[node].dep_items) {
+                waiting = node + 1u;
+                continue;
+            }
+            const unsigned mine = atomicAdd(heads + l, 1u);
+            if (mine < len) {
+                lane0 = l;
+                return r.x + mine;
+            }
         }
         if (finished == e.nlanes) return kNoItem;
         if (t0 == 0) {
@@ -1589,8 +1610,14 @@ __global__ void __launch_bounds__(kPersThreads, 2)
     unsigned lane0 = e.nlanes ? blockIdx.x % e.nlanes : 0u; // thread 0's scan start
     for (;;) {
         if (tid == 0) {
-            s_item = pers_claim(e, lane0);
-            __threadfence(); // the claimed item's inputs (acquired above) before the body's loads
+            const unsigned i = pers_claim(e, lane0);
+            s_item = i;
+            if (i != kNoItem) {
+                const unsigned node = e.items[i].node;
+                const int dep = e.nodes[node].dep;
+                if (dep >= 0) pers_wait(e, node, dep, e.nodes[node].dep_items);
+            }
+            __threadfence(); // the item's inputs (acquired above) before the body's loads
         }
         __syncthreads();
         const unsigned i = s_item;
