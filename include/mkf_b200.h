@@ -310,12 +310,11 @@ typedef struct mkf_batch mkf_batch;
 #define MKF_BATCH_FUSE_KEYS 2
 /* Run the whole plan as ONE launch of a persistent executor: the plan
  * records every lane's kernel launches (grid and arguments) instead of
- * issuing them; each lane becomes a queue of (launch, block range) items in
- * device memory, and one CTA per resident slot (two 512-thread CTAs per SM)
- * repeatedly claims, from any lane, the next item whose launch may start
- * (the launch before it in the lane has finished) and runs the recorded
- * kernel's body on its blocks (256-thread bodies two to a CTA).  Waiting
- * for ready work is bounded (2 s); a wait that runs out marks the plan
+ * issuing them, and one CTA per resident slot (two 512-thread CTAs per SM)
+ * takes (launch, block range) items from a queue in device memory, waits
+ * until the launch before its own in the same lane has finished, and runs
+ * the recorded kernel's body on its blocks (256-thread bodies two to a
+ * CTA).  Every wait is bounded (2 s); a wait that runs out marks the plan
  * failed (mkf_batch_check) and the launch still ends.  Available for
  * MKF-CKKS jobs on rings of logN 13-16; a plan whose jobs launch anything
  * the executor cannot run is refused (MKF_ERR_INVALID_ARG).  Combines with

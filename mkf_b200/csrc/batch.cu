@@ -164,11 +164,10 @@ struct mkf_batch {
     bool persistent = false;
     PNode *d_nodes = nullptr;
     PItem *d_items = nullptr;
-    uint2 *d_lanes = nullptr;
     unsigned char *d_blob = nullptr;
     unsigned *d_ctl = nullptr;
     size_t ctl_bytes = 0;
-    unsigned nitems = 0, nnodes = 0, nlanes = 0;
+    unsigned nitems = 0, nnodes = 0;
     unsigned long long wait_ns = 0;
     cudaStream_t last_stream = nullptr;
     // the lane scratch buffers a graph or persistent plan recorded addresses in
@@ -268,26 +267,23 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
             n.vpi = std::max(1u, std::min(64u, slots / (4 * ncta)));
             n.items = (slots + n.vpi - 1) / n.vpi;
         }
-    // nodes and items lane by lane: node j of a lane waits for node j-1 of
-    // the same lane, and a lane's items are one contiguous queue
     std::vector<PNode> nodes;
     std::vector<PItem> items;
-    std::vector<uint2> lanes;
-    for (auto &ln : rec.lanes) {
-        if (ln.empty()) continue;
-        const unsigned first = (unsigned)items.size();
-        int prev = -1;
-        for (PNode n : ln) {
-            n.dep = prev;
-            n.dep_items = prev >= 0 ? nodes[prev].items : 0;
+    std::vector<int> prev(rec.lanes.size(), -1);
+    size_t longest = 0;
+    for (auto &ln : rec.lanes) longest = std::max(longest, ln.size());
+    for (size_t pos = 0; pos < longest; ++pos)
+        for (size_t l = 0; l < rec.lanes.size(); ++l) {
+            if (pos >= rec.lanes[l].size()) continue;
+            PNode n = rec.lanes[l][pos];
+            n.dep = prev[l];
+            n.dep_items = prev[l] >= 0 ? nodes[prev[l]].items : 0;
             const unsigned id = (unsigned)nodes.size();
-            prev = (int)id;
+            prev[l] = (int)id;
             const unsigned per = (n.threads == kPersThreads ? 1u : 2u) * n.vpi;
             for (unsigned i = 0; i < n.items; ++i) items.push_back(PItem{id, i * per});
             nodes.push_back(n);
         }
-        lanes.push_back(make_uint2(first, (unsigned)items.size()));
-    }
     b->wait_ns = 2000000000ull; // 2 s: one stage of one product takes milliseconds
     if ((flags & MKF_BATCH_TEST_STALL) && !nodes.empty() && nodes.back().dep >= 0) {
         nodes.back().dep_items += 1; // a count nothing reaches: the wait runs out
@@ -295,11 +291,9 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
     }
     b->nnodes = (unsigned)nodes.size();
     b->nitems = (unsigned)items.size();
-    b->nlanes = (unsigned)lanes.size();
-    b->ctl_bytes = sizeof(unsigned) * (kCtlDone0 + nodes.size() + lanes.size() + 1);
+    b->ctl_bytes = sizeof(unsigned) * (kCtlDone0 + std::max<size_t>(nodes.size(), 1));
     if (cudaMalloc(&b->d_nodes, sizeof(PNode) * std::max<size_t>(nodes.size(), 1)) != cudaSuccess ||
         cudaMalloc(&b->d_items, sizeof(PItem) * std::max<size_t>(items.size(), 1)) != cudaSuccess ||
-        cudaMalloc(&b->d_lanes, sizeof(uint2) * std::max<size_t>(lanes.size(), 1)) != cudaSuccess ||
         cudaMalloc(&b->d_blob, std::max<size_t>(rec.blob.size(), 16)) != cudaSuccess ||
         cudaMalloc(&b->d_ctl, b->ctl_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -307,7 +301,6 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
     }
     if (!nodes.empty()) cudaMemcpy(b->d_nodes, nodes.data(), sizeof(PNode) * nodes.size(), cudaMemcpyHostToDevice);
     if (!items.empty()) cudaMemcpy(b->d_items, items.data(), sizeof(PItem) * items.size(), cudaMemcpyHostToDevice);
-    if (!lanes.empty()) cudaMemcpy(b->d_lanes, lanes.data(), sizeof(uint2) * lanes.size(), cudaMemcpyHostToDevice);
     if (!rec.blob.empty()) cudaMemcpy(b->d_blob, rec.blob.data(), rec.blob.size(), cudaMemcpyHostToDevice);
     cudaMemset(b->d_ctl, 0, b->ctl_bytes);
     b->persistent = true;
@@ -318,7 +311,7 @@ mkf_status build_persistent(mkf_batch *b, int flags) {
 // One run of the persistent plan on st: reset the queue, launch the executor.
 mkf_status issue_persistent(mkf_batch *b, cudaStream_t st) {
     cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st);
-    PExec e{b->d_nodes, b->d_items, b->d_lanes, b->d_blob, b->nlanes, b->nnodes, b->d_ctl, b->wait_ns};
+    PExec e{b->d_nodes, b->d_items, b->d_blob, b->nitems, b->d_ctl, b->wait_ns};
     if (b->nitems && launch_persistent(e, b->device, st) == 0)
         return fail(b->ctx, MKF_ERR_CUDA, "persistent executor launch failed");
     return cuda_check(b->ctx, "persistent executor launch");
@@ -523,8 +516,8 @@ mkf_status mkf_batch_check(mkf_batch *b) {
         return fail(b->ctx, MKF_ERR_CUDA, "cannot read the executor's control words");
     if (w[kCtlError])
         return fail(b->ctx, MKF_ERR_TIMEOUT,
-                    "persistent plan: no recorded launch became ready within the wait bound (node " +
-                        std::to_string((long long)w[kCtlStalled] - 1) + " was waiting); the plan's outputs are not valid");
+                    "persistent plan: the wait of node " + std::to_string((long long)w[kCtlStalled] - 1) +
+                        " ran out; the plan's outputs are not valid");
     return MKF_OK;
 }
 
@@ -541,7 +534,6 @@ void mkf_batch_destroy(mkf_batch *b) {
         if (e) cudaEventDestroy(e);
     if (b->d_nodes) cudaFree(b->d_nodes);
     if (b->d_items) cudaFree(b->d_items);
-    if (b->d_lanes) cudaFree(b->d_lanes);
     if (b->d_blob) cudaFree(b->d_blob);
     if (b->d_ctl) cudaFree(b->d_ctl);
     delete b;

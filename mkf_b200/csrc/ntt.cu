@@ -1526,8 +1526,8 @@ MKF_DEV unsigned long long global_ns() {
 
 // Waits until node dep has finished `need` items (thread 0 of the CTA).
 // Bounded by e.wait_ns of the global timer and by an iteration count; past
-// either, or once another wait has run out, it raises the error flag, notes
-// the node that gave up, and returns.
+// either, or once another wait has expired, it raises the error flag, notes
+// the first node that gave up, and returns.
 MKF_DEV void pers_wait(const PExec &e, unsigned node, int dep, unsigned need) {
     const unsigned *c = e.ctl + kCtlDone0 + dep;
     if (ld_acquire_u32(c) >= need) return;
@@ -1545,57 +1545,6 @@ MKF_DEV void pers_wait(const PExec &e, unsigned node, int dep, unsigned need) {
     }
 }
 
-// Claims for this CTA (thread 0) the next item of a lane whose head launch
-// may start (the launch before it in the lane has finished all its items):
-// the lanes are scanned from the one this CTA last took an item from, and
-// the claim is an atomic add on that lane's head, so it may land on the
-// next launch of the lane, which the caller then waits for (pers_wait).  A
-// lane whose head launch cannot start is passed over, so no CTA holds an
-// item behind another lane's unfinished work.  Returns the item, or kNoItem
-// when every lane is finished.  When no lane can start, the wait is bounded
-// like pers_wait's.
-constexpr unsigned kNoItem = 0xffffffffu;
-MKF_DEV unsigned pers_claim(const PExec &e, unsigned &lane0) {
-    unsigned *heads = e.ctl + kCtlDone0 + e.nnodes;
-    unsigned long long t0 = 0;
-    unsigned back = 32;
-    for (int it = 0;; ++it) {
-        if (ld_acquire_u32(e.ctl + kCtlError) != 0u) return kNoItem;
-        unsigned finished = 0, waiting = 0;
-        for (unsigned j = 0; j < e.nlanes; ++j) {
-            const unsigned l = lane0 + j < e.nlanes ? lane0 + j : lane0 + j - e.nlanes;
-            // the lane's items are [r.x, r.y); its head counts the ones claimed
-            const uint2 r = e.lanes[l];
-            const unsigned len = r.y - r.x;
-            const unsigned h = ld_acquire_u32(heads + l);
-            if (h >= len) {
-                ++finished;
-                continue;
-            }
-            const unsigned node = e.items[r.x + h].node;
-            const int dep = e.nodes[node].dep;
-            if (dep >= 0 && ld_acquire_u32(e.ctl + kCtlDone0 + dep) < e.nodes[node].dep_items) {
-                waiting = node + 1u;
-                continue;
-            }
-            const unsigned mine = atomicAdd(heads + l, 1u);
-            if (mine < len) {
-                lane0 = l;
-                return r.x + mine;
-            }
-        }
-        if (finished == e.nlanes) return kNoItem;
-        if (t0 == 0) {
-            t0 = global_ns();
-        } else if (global_ns() - t0 > e.wait_ns || it >= (1 << 24)) {
-            if (atomicExch(e.ctl + kCtlError, 1u) == 0u) atomicExch(e.ctl + kCtlStalled, waiting);
-            return kNoItem;
-        }
-        __nanosleep(back);
-        back = back < 1024 ? 2 * back : back;
-    }
-}
-
 MKF_DEV VBlk pers_vblk(const PNode &nd, unsigned vb, unsigned t, unsigned bar, unsigned nt,
                        uint64_t *sm) {
     const unsigned x = vb % nd.gx, yz = vb / nd.gx;
@@ -1607,23 +1556,18 @@ __global__ void __launch_bounds__(kPersThreads, 2)
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ unsigned s_item;
     const unsigned tid = threadIdx.x;
-    unsigned lane0 = e.nlanes ? blockIdx.x % e.nlanes : 0u; // thread 0's scan start
     for (;;) {
-        if (tid == 0) {
-            const unsigned i = pers_claim(e, lane0);
-            s_item = i;
-            if (i != kNoItem) {
-                const unsigned node = e.items[i].node;
-                const int dep = e.nodes[node].dep;
-                if (dep >= 0) pers_wait(e, node, dep, e.nodes[node].dep_items);
-            }
-            __threadfence(); // the item's inputs (acquired above) before the body's loads
-        }
+        if (tid == 0) s_item = atomicAdd(e.ctl + kCtlHead, 1u);
         __syncthreads();
         const unsigned i = s_item;
-        if (i == kNoItem) return;
+        if (i >= e.nitems) return;
         const PItem it = e.items[i];
         const PNode nd = e.nodes[it.node];
+        if (tid == 0 && nd.dep >= 0) {
+            pers_wait(e, it.node, nd.dep, nd.dep_items);
+            __threadfence();
+        }
+        __syncthreads();
         if (nd.threads == kPersThreads) {
             for (unsigned j = 0; j < nd.vpi; ++j) {
                 const unsigned vb = it.vb0 + j;

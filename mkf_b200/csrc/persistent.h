@@ -1,10 +1,9 @@
 // Persistent batch plans: the kernels of every product of a batch plan run
 // as one launch of a persistent executor.  The plan records each lane's
-// launches (kernel, grid, arguments) instead of issuing them; each lane
-// becomes a queue of (launch, block range) items in device memory, and the
-// executor's CTAs claim, from any lane, the next item whose launch may start
-// (the launch before it in the lane has finished every item), run the
-// launch's kernel body on it and count it done.
+// launches (kernel, grid, arguments) instead of issuing them; the executor's
+// CTAs take (launch, block range) items from a queue in device memory and run
+// the launch's kernel body on them, waiting (bounded) until the launch before
+// it in the same lane has finished every item.
 #pragma once
 
 #include "common.cuh"
@@ -52,18 +51,16 @@ struct PItem {
                         // item runs vb0 .. vb0+vpi-1, the halves of a
                         // 256-thread item vb0+h, vb0+h+2, ... (h = 0, 1)
 };
-// Control words: [0] unused, [1] error flag, [2] the node a CTA was waiting
-// for when its wait ran out + 1, [3] unused, then one finished-item counter
-// per node, then one queue head per lane.
-constexpr int kCtlError = 1, kCtlStalled = 2, kCtlDone0 = 4;
+// Control words: [0] queue head, [1] error flag, [2] first node whose wait
+// expired + 1, [3] unused, then one finished-item counter per node.
+constexpr int kCtlHead = 0, kCtlError = 1, kCtlStalled = 2, kCtlDone0 = 4;
 struct PExec {
     const PNode *nodes;
     const PItem *items;
-    const uint2 *lanes;  // per lane: its items [x, y) (a lane's items are contiguous)
     const unsigned char *blob;
-    unsigned nlanes, nnodes;
+    unsigned nitems;
     unsigned *ctl;
-    unsigned long long wait_ns; // bound of a CTA's wait for ready work
+    unsigned long long wait_ns; // bound of one wait
 };
 
 // Arguments of the executor's own bodies: recorded copies and fills.
