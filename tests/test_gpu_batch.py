@@ -290,3 +290,33 @@ def test_plan_keeps_its_scratch_when_a_later_plan_grows_the_lanes(rings, persist
             assert np.array_equal(j[4].download(), want[i]), f"job {i} differs"
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("log_n,row_log", [(15, 0), (15, 7), (16, 0), (14, 8)])
+def test_persistent_batch_on_larger_rings_and_splits(log_n, row_log):
+    """The executor's bodies for every phase shape: rings of logN 14-16 with
+    their default and other NTT split, a few products of uneven party count
+    and level, one persistent launch, each output equal to its single call."""
+    lit = params.small("ckks", log_n=log_n, n_q=5, n_p=2, q_bits=45, first_bits=55, p_bits=55,
+                       scale_bits=45)
+    P = ev.Parameters(lit, "ckks", ntt_row_log=row_log)
+    g = np.random.default_rng(log_n * 10 + row_log)
+    qp = list(lit.q) + list(lit.p)
+    beta = (len(lit.q) - 1 + len(lit.p)) // len(lit.p)
+    jobs, singles = [], []
+    for k, level, mat in [(2, lit.max_level, True), (3, 2, False)]:
+        keys = ev.MKFKeySet(P, [np.ascontiguousarray(_limbs(g, qp, lit.n, (beta, 2))) for _ in range(k)],
+                            np.ascontiguousarray(_limbs(g, qp, lit.n, (beta, 2))))
+        E = ev.MKFEvaluator(P, keys)
+        left, right = (ev.Ciphertext.from_array(P, _limbs(g, lit.q[: level + 1], lit.n, (k + 1,)), True,
+                                                scale=lit.scale) for _ in range(2))
+        out = ev.Ciphertext(P, k + 1 if mat else 2, E.output_level(left, right, True), True)
+        jobs.append(("mkf", E, left, right, out, True, mat))
+        singles.append(lambda E=E, l=left, r=right, m=mat: E.MulRelinNew(l, r, True, m).download())
+    want = [f() for f in singles]
+    b = ev.Batch(P, jobs, lanes=2, graph=True, persistent=True)
+    b.launch()
+    b.check()
+    for i, j in enumerate(jobs):
+        assert np.array_equal(j[4].download(), want[i]), f"job {i} differs (logN {log_n}, row_log {row_log})"
+    b.close()
