@@ -368,7 +368,7 @@ MKF_DEV void ip_body(const B &bk, const IpArgs &a, const DevModulus *mods, int N
 
 // The stand-alone kernels (kernels.cu), declared for the persistent
 // executor, which reads their recorded arguments back in their own types.
-__global__ void __launch_bounds__(kBlock) digits_prep_kernel(const uint64_t *in, long long in_pstride,
+__global__ void __launch_bounds__(kBlock, 4) digits_prep_kernel(const uint64_t *in, long long in_pstride,
                                                              const ModUpTab *tabs, const DevModulus *mods,
                                                              uint64_t *y, uint8_t *v, int level, int alpha,
                                                              int ndigits, int N, int n1, int n2);
