@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--profile-products", type=int, default=0,
                     help="profiling run: after --warmup products, run this many plain products of "
                          "the headline workload (one stream) and exit; for ncu captures")
+    ap.add_argument("--profile-persistent", action="store_true",
+                    help="with --profile-products: run them as one persistent plan instead")
     ap.add_argument("--configs", type=int, default=1,
                     help="1: also time C1 and C2 (plain GPU, oracle on one core)")
     ap.add_argument("--serve-only", action="store_true",
@@ -434,11 +436,24 @@ def run_c3(a, reps, ws, rank, local):
     max_over_ranks = reps.max_over_ranks
 
     if a.profile_products > 0:
-        for i in range(a.warmup):
-            product(i, streams[0])
-        torch.cuda.synchronize()
-        for i in range(a.profile_products):
-            product(i, streams[0])
+        if a.profile_persistent:
+            # the products as one persistent plan (one lane), launched
+            # --warmup times and then once more
+            pouts = [ev.Ciphertext(P, k + 1, lout, True) for _ in range(a.profile_products)]
+            pj = [("mkf", E, ins[j % nin][0], ins[j % nin][1], pouts[j], True, True)
+                  for j in range(a.profile_products)]
+            plan = ev.Batch(P, pj, lanes=1, graph=False, persistent=True)
+            cs0 = ctypes_stream(streams[0])
+            for _ in range(a.warmup + 1):
+                plan.launch(cs0)
+            plan.check()
+            plan.close()
+        else:
+            for i in range(a.warmup):
+                product(i, streams[0])
+            torch.cuda.synchronize()
+            for i in range(a.profile_products):
+                product(i, streams[0])
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"profile_products": a.profile_products, "tuning": tuned["best"],
