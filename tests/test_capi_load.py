@@ -41,3 +41,31 @@ def test_ctx_create_without_gpu_fails_cleanly():
     from mkf_b200.evaluator import Parameters
     with pytest.raises(capi.MKFError):
         Parameters(params.small("ckks", 10, 3, 2), "ckks")
+
+
+def test_python_constants_match_the_header():
+    """The Python binding's copies of the header's constants (status codes,
+    flags, job kinds, batch flags, slot ops) have the header's values, and
+    the parameter descriptor has the header's fields in order."""
+    import re
+    from mkf_b200 import capi
+    text = open(capi.HEADER).read()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (MKF_\w+) (\d+)", text)}
+    enums = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(MKF_(?:ERR_\w+|OK|FLAG_\w+))\s*=\s*(\d+)", text)}
+    for name, value in enums.items():
+        if name.startswith("MKF_ERR_") or name == "MKF_OK":
+            assert capi.STATUS[value] == name
+    assert capi.FLAG_RESCALE == enums["MKF_FLAG_RESCALE"]
+    assert capi.FLAG_MATERIALIZE == enums["MKF_FLAG_MATERIALIZE"]
+    for short in ("BATCH_GRAPH", "BATCH_FUSE_KEYS", "BATCH_PERSISTENT", "BATCH_TEST_STALL",
+                  "JOB_MKF", "JOB_KKLSS", "SLOT_MUL_ADD", "SLOT_ADD_C0", "SLOT_MUL"):
+        assert getattr(capi, short) == defines["MKF_" + short], short
+    for cname, pycls in (("mkf_params_desc", capi.ParamsDesc), ("mkf_tuning", capi.Tuning),
+                         ("mkf_job", capi.Job), ("mkf_server_config", capi.ServerConfig)):
+        body = text[text.index("typedef struct %s {" % cname):text.index("} %s;" % cname)]
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = []
+        for decl in re.findall(r"([^;{]+);", body):
+            # "const mkf_ct *a, *b" declares two fields
+            fields += [re.split(r"[\s*]+", part.strip())[-1] for part in decl.split(",")]
+        assert fields == [f for f, _ in pycls._fields_], cname
